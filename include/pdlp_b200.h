@@ -1,0 +1,213 @@
+/*
+ * pdlp_b200 -- C ABI of the B200-native PDLP engine.
+ *
+ * This library replaces, for the `--method pdlp` path of sovopt
+ * (manabsen006-a11y/Sovereign-MOE), two reference interfaces:
+ *
+ *   1. the solver entry point  solve_pdlp(prob, params) -> Solution
+ *      (src/sovopt/lp/pdlp.py:238-494, parameters pdlp.py:79-116,
+ *      info pdlp.py:119-132), and
+ *   2. the kernel-level Backend the solver is written against
+ *      (src/sovopt/core/backend.py:317-493: spmv, primal_step, dual_step,
+ *      pdhg_primal, pdhg_dual, pdhg_accum, dot, nrm2, nrm_inf).
+ *
+ * Conventions
+ *   - Every call returns int: 0 on success, a negative PDLP_ERR_* code on
+ *     failure; pdlp_last_error() gives a thread-local message.
+ *   - Pointers are plain device pointers unless a `memory` argument says
+ *     PDLP_MEM_HOST.  The library never frees memory it did not allocate; it
+ *     owns only its handles' scratch.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *   - A handle (pdlp_batch) is used from one host thread at a time.
+ *   - Sparse matrices use the reference's storage (src/sovopt/core/sparse.py:
+ *     263-298): int64 pointers, int32 indices, float64 values, held in both
+ *     CSR (rows) and CSC (columns).
+ */
+#ifndef PDLP_B200_H
+#define PDLP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PDLP_ABI_VERSION 1
+
+/* ---- error codes ------------------------------------------------------- */
+#define PDLP_OK                   0
+#define PDLP_ERR_ARG             -1   /* invalid argument / malformed input   */
+#define PDLP_ERR_OOM             -2   /* device memory does not fit           */
+#define PDLP_ERR_CUDA            -3   /* a CUDA runtime call failed           */
+#define PDLP_ERR_BARRIER_TIMEOUT -4   /* a bounded device wait gave up        */
+#define PDLP_ERR_NUMERICAL       -5   /* non-finite input data                */
+#define PDLP_ERR_STATE           -6   /* call not valid in the handle's state */
+
+/* ---- statuses: same integers as sovopt Status (src/sovopt/core/problem.py:58-69) */
+#define PDLP_STATUS_OPTIMAL          0
+#define PDLP_STATUS_ITERATION_LIMIT  4
+#define PDLP_STATUS_TIME_LIMIT       5
+#define PDLP_STATUS_NUMERICAL        8
+#define PDLP_STATUS_INTERRUPTED      9
+#define PDLP_STATUS_RUNNING         -1
+
+#define PDLP_MEM_DEVICE 0
+#define PDLP_MEM_HOST   1
+
+/* scaling methods (params.scaling of pdlp.py:113; scaling.py:312-318) */
+#define PDLP_SCALING_PDLP            0   /* Ruiz (10) then Pock-Chambolle, pow2 */
+#define PDLP_SCALING_NONE            1
+#define PDLP_SCALING_RUIZ            2   /* Ruiz (20), pow2                     */
+#define PDLP_SCALING_POCK_CHAMBOLLE  3
+
+/* One LP in the reference's row-bounds form rl <= Ax <= ru, l <= x <= u
+ * (src/sovopt/core/problem.py:81-128).  Infinite bounds are +-1e30. */
+typedef struct pdlp_problem_desc {
+    int32_t m, n;
+    int64_t nnz;
+    const int64_t* rp; const int32_t* ri; const double* rx;   /* CSR of A */
+    const int64_t* cp; const int32_t* ci; const double* cx;   /* CSC of A */
+    const double* c;
+    const double* row_lb; const double* row_ub;
+    const double* col_lb; const double* col_ub;
+    const uint8_t* kind;        /* optional (NULL): VarKind per column; non-zero
+                                   columns keep a scale factor of 1         */
+    double obj_offset;
+    int32_t sense;              /* 1 minimise, -1 maximise (ObjSense)       */
+    int32_t memory;             /* PDLP_MEM_DEVICE or PDLP_MEM_HOST          */
+} pdlp_problem_desc;
+
+/* PDLPParams (src/sovopt/lp/pdlp.py:79-116), same names and defaults. */
+typedef struct pdlp_params {
+    double eps_abs, eps_rel, feas_cap;
+    int64_t max_iter;
+    double time_limit;                  /* seconds, measured from admission  */
+    int32_t check_every, stepsize_every;
+    double beta_sufficient, beta_necessary, beta_artificial;
+    double primal_weight_smoothing;
+    int32_t scaling;                    /* PDLP_SCALING_*                    */
+    const double* power_start;          /* optional n-vector (memory as the
+                                           problem) starting the power
+                                           iteration for ||A||_2 (pdlp.py:
+                                           140-159 uses default_rng(0)); NULL:
+                                           a fixed device-generated vector   */
+    double time_used;                   /* seconds already spent by the caller
+                                           (counts against time_limit)       */
+    int32_t history_capacity;           /* checks recorded (0 = none)        */
+} pdlp_params;
+
+void pdlp_params_default(pdlp_params* p);
+
+/* Result of one solve: PDLPInfo (pdlp.py:119-132) plus the Solution scalars. */
+typedef struct pdlp_result {
+    int32_t status;
+    int64_t iterations, restarts, rejected_steps;
+    double primal_res, dual_res, gap, primal_obj, dual_obj;  /* NaN unless OPTIMAL */
+    double step_size, primal_weight;
+    double objective;              /* c'x + offset of the returned point       */
+    double scale_obj;              /* objective scale of the preconditioner    */
+    int32_t history_len;           /* checks recorded in the history buffer    */
+    double device_seconds;         /* engine time for this LP on the device    */
+} pdlp_result;
+
+/* ---- library ---------------------------------------------------------- */
+int pdlp_abi_version(void);
+const char* pdlp_last_error(void);
+
+/* ---- whole solve: solve_pdlp (pdlp.py:238-494) ------------------------- *
+ * Solves one LP: scaling, PDHG, restarts and termination all run on the
+ * device.  x (n), y (m), reduced_costs (n) receive the unscaled solution with
+ * the reference's conventions (y textbook sign, d = c - A'y, x clipped to its
+ * bounds); any of them may be NULL.  history (optional, 5*capacity doubles)
+ * receives (k, primal_res, dual_res, gap, primal_obj) per check.  All output
+ * pointers live in `out_memory`. */
+int pdlp_solve(const pdlp_problem_desc* prob, const pdlp_params* params,
+               void* stream, pdlp_result* result,
+               double* x, double* y, double* reduced_costs, double* history,
+               int32_t out_memory);
+
+/* ---- batched / served engine ------------------------------------------- *
+ * A batch holds device-resident LPs ("slots") that one persistent kernel
+ * advances together, each with its own step size, primal weight, restart
+ * state and termination.  LPs may be admitted and retired between steps. */
+typedef struct pdlp_batch pdlp_batch;
+
+typedef struct pdlp_batch_config {
+    int32_t max_slots;          /* capacity of the slot table               */
+    int32_t persistent;         /* 1: one cooperative launch per call to
+                                   pdlp_batch_step; 0: one launch per phase
+                                   (replayed from a CUDA graph)             */
+    int32_t block_threads;      /* 0 = default (256)                        */
+    int32_t tile_rows;          /* 0 = default                              */
+    int32_t tile_nnz;           /* 0 = default                              */
+    int32_t lanes_override;     /* 0 = per-LP choice; else lanes per row    */
+    int64_t memory_budget;      /* bytes the batch may hold; 0 = free HBM   */
+} pdlp_batch_config;
+
+void pdlp_batch_config_default(pdlp_batch_config* cfg);
+int pdlp_batch_create(const pdlp_batch_config* cfg, void* stream, pdlp_batch** out);
+int pdlp_batch_destroy(pdlp_batch* b);
+/* Copies (host or device) and preconditions one LP into a free slot.
+ * Returns PDLP_ERR_OOM when it does not fit the memory budget, leaving the
+ * batch unchanged. */
+int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* prob,
+                     const pdlp_params* params, int32_t* slot_out);
+/* Advances every active slot by up to `max_steps` engine steps (a step is one
+ * half-iteration pair: the A pass and the A^T pass).  *active_out receives the
+ * number of slots still running. */
+int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out);
+/* Status and info of a slot (status PDLP_STATUS_RUNNING while running). */
+int pdlp_batch_poll(pdlp_batch* b, int32_t slot, pdlp_result* result);
+/* Copies a finished slot's solution out (pointers in `memory`; NULL skips). */
+int pdlp_batch_fetch(pdlp_batch* b, int32_t slot, double* x, double* y,
+                     double* reduced_costs, double* history, int32_t memory);
+/* Releases a slot's device memory. */
+int pdlp_batch_retire(pdlp_batch* b, int32_t slot);
+/* Requests the slot to stop at its next check (status INTERRUPTED). */
+int pdlp_batch_cancel(pdlp_batch* b, int32_t slot);
+/* Device bytes a slot for this problem would take (admission planning). */
+int64_t pdlp_slot_bytes(int32_t m, int32_t n, int64_t nnz);
+/* Per-kernel timing of the last pdlp_batch_step: total device milliseconds
+ * and algorithmic bytes moved by the PDHG iterations. */
+int pdlp_batch_last_timing(pdlp_batch* b, double* ms, double* iter_bytes,
+                           int64_t* iterations);
+
+/* ---- kernel-level Backend (backend.py:317-493) -------------------------- *
+ * Device pointers; `stream` as above.  FP64 unless named _f32. */
+
+/* y = A x, A in CSR with int64 pointers (backend.py:373-384) */
+int pdlp_spmv_f64(int32_t m, const int64_t* rp, const int32_t* ri, const double* rx,
+                  const double* x, double* y, void* stream);
+int pdlp_spmv_f32(int32_t m, const int64_t* rp, const int32_t* ri, const float* rx,
+                  const float* x, float* y, void* stream);
+/* Y = A X, X dense (ncols, k) row-major, batch index fastest (backend.py:386-400) */
+int pdlp_spmm_f64(int32_t m, int32_t k, const int64_t* rp, const int32_t* ri,
+                  const double* rx, const double* X, double* Y, void* stream);
+/* xnew = clamp(x - tau (c + aty), lo, hi) (backend.py:404-415) */
+int pdlp_primal_step(int32_t n, double* xnew, const double* x, const double* c,
+                     const double* aty, const double* lo, const double* hi,
+                     double tau, void* stream);
+/* ynew = w - sigma clamp(w / sigma, rl, ru), w = y + sigma ax (backend.py:417-434) */
+int pdlp_dual_step(int32_t m, double* ynew, const double* y, const double* ax,
+                   const double* rl, const double* ru, double sigma, void* stream);
+/* x <- clamp(x - tau (c + aty), lo, hi), dx = xnew - xold (backend.py:441-452) */
+int pdlp_pdhg_primal(int32_t n, double* x, double* dx, const double* c,
+                     const double* aty, const double* lo, const double* hi,
+                     double tau, void* stream);
+/* ax += adx; w = y + sigma (ax + adx); y <- prox; dy (backend.py:454-467) */
+int pdlp_pdhg_dual(int32_t m, double* y, double* dy, double* ax, const double* adx,
+                   const double* rl, const double* ru, double sigma, void* stream);
+/* acc += inc; sum += eta v (backend.py:469-479) */
+int pdlp_pdhg_accum(int32_t n, double* acc, const double* inc, double* run_sum,
+                    const double* v, double eta, void* stream);
+/* Reductions to a host double (synchronising, like the reference's float()
+ * conversions, backend.py:483-490).  Deterministic: a fixed reduction tree. */
+int pdlp_dot(int64_t n, const double* a, const double* b, double* out, void* stream);
+int pdlp_nrm2(int64_t n, const double* a, double* out, void* stream);
+int pdlp_nrm_inf(int64_t n, const double* a, double* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PDLP_B200_H */

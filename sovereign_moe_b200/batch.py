@@ -1,0 +1,142 @@
+"""Batched engine: many LPs advanced together by one persistent kernel.
+
+``BatchEngine`` wraps the ``pdlp_batch_*`` entry points of ``libpdlp_b200.so``.
+LPs are admitted into slots (their data is copied to the device and
+preconditioned there), every ``step`` advances all running slots, and a
+finished slot's unscaled solution is fetched and the slot retired.  Each LP
+keeps its own step size, primal weight, restart state and termination, and
+its per-LP reductions run over its own tiles only, so its result does not
+depend on which other LPs share the launch.
+
+The reference has no batched PDLP (its only batched first-order method is the
+shared-matrix node relaxation of ``src/sovopt/mip/bnr.py:176-301``); the
+per-LP algorithm is exactly ``solve_pdlp``'s.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import time
+
+import numpy as np
+
+from . import _lib
+from .pdlp import PDLPParams, _check_device, _to_solution, params_struct, problem_desc
+
+__all__ = ["BatchEngine"]
+
+
+class BatchEngine:
+    """A slot table of device-resident LPs and the engine that advances them."""
+
+    def __init__(self, max_slots=256, persistent=True, tile_rows=0, tile_nnz=0,
+                 lanes_override=0, memory_budget=0, stream=None):
+        self.lib = _lib.load()
+        cfg = _lib.BatchConfig()
+        self.lib.pdlp_batch_config_default(ctypes.byref(cfg))
+        cfg.max_slots = int(max_slots)
+        cfg.persistent = 1 if persistent else 0
+        if tile_rows:
+            cfg.tile_rows = int(tile_rows)
+        if tile_nnz:
+            cfg.tile_nnz = int(tile_nnz)
+        cfg.lanes_override = int(lanes_override)
+        cfg.memory_budget = int(memory_budget)
+        h = ctypes.c_void_p()
+        code = self.lib.pdlp_batch_create(ctypes.byref(cfg), stream, ctypes.byref(h))
+        if code == _lib.PDLP_ERR_CUDA:
+            raise RuntimeError(f"GPU backend unavailable ({self.lib.pdlp_last_error().decode()})")
+        _lib.check(code)
+        self.h = h
+        self.max_slots = int(max_slots)
+        self._meta = {}
+
+    def close(self):
+        if self.h:
+            self.lib.pdlp_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- slots ------------------------------------------------------------- #
+
+    def admit(self, prob, params: PDLPParams | None = None, power_start="reference"):
+        """Copy ``prob`` to the device and precondition it; returns the slot.
+        Raises ``PDLPError`` with code ``PDLP_ERR_OOM`` when it does not fit."""
+        params = params or PDLPParams()
+        _check_device(params.device)
+        t0 = time.perf_counter()
+        desc, keep = problem_desc(prob)
+        p, keep_v0 = params_struct(params, int(prob.A.n), power_start=power_start)
+        slot = ctypes.c_int32(-1)
+        _lib.check(self.lib.pdlp_batch_admit(self.h, ctypes.byref(desc), ctypes.byref(p),
+                                             ctypes.byref(slot)))
+        del keep, keep_v0
+        self._meta[slot.value] = (prob, params, int(p.history_capacity), t0)
+        return slot.value
+
+    def step(self, max_steps=1 << 16):
+        """Advance every running slot; returns how many are still running."""
+        active = ctypes.c_int32(0)
+        _lib.check(self.lib.pdlp_batch_step(self.h, int(max_steps), ctypes.byref(active)))
+        return active.value
+
+    def run(self, chunk=1 << 16):
+        """Step until no slot is running."""
+        while self.step(chunk) > 0:
+            pass
+
+    def poll(self, slot):
+        r = _lib.Result()
+        _lib.check(self.lib.pdlp_batch_poll(self.h, int(slot), ctypes.byref(r)))
+        return r
+
+    def done(self, slot):
+        return self.poll(slot).status != _lib.PDLP_STATUS_RUNNING
+
+    def fetch(self, slot):
+        """The finished slot's result as a reference ``Solution``."""
+        prob, params, hcap, t0 = self._meta[slot]
+        r = self.poll(slot)
+        m, n = int(prob.A.m), int(prob.A.n)
+        x, y, d = np.empty(n), np.empty(m), np.empty(n)
+        hist = np.empty(5 * max(hcap, 1))
+        _lib.check(self.lib.pdlp_batch_fetch(self.h, int(slot), x.ctypes.data, y.ctypes.data,
+                                             d.ctypes.data, hist.ctypes.data, _lib.PDLP_MEM_HOST))
+        return _to_solution(prob, params, r, x, y, d, hist, time.perf_counter() - t0)
+
+    def retire(self, slot):
+        _lib.check(self.lib.pdlp_batch_retire(self.h, int(slot)))
+        self._meta.pop(slot, None)
+
+    def cancel(self, slot):
+        _lib.check(self.lib.pdlp_batch_cancel(self.h, int(slot)))
+
+    def last_timing(self):
+        """(device ms, algorithmic PDHG bytes, PDHG iterations) of the last step."""
+        ms, by, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
+        _lib.check(self.lib.pdlp_batch_last_timing(self.h, ctypes.byref(ms), ctypes.byref(by),
+                                                   ctypes.byref(it)))
+        return ms.value, by.value, it.value
+
+    def slot_bytes(self, m, n, nnz):
+        return int(self.lib.pdlp_slot_bytes(int(m), int(n), int(nnz)))
+
+    def solve_all(self, probs, params=None):
+        """Admit every LP, run to completion, fetch and retire: list of Solutions."""
+        slots = [self.admit(p, params) for p in probs]
+        self.run()
+        out = [self.fetch(s) for s in slots]
+        for s in slots:
+            self.retire(s)
+        return out

@@ -1,0 +1,810 @@
+// PDLP engine: kernels (persistent cooperative and per-pass) and the batch
+// runtime behind the C ABI (admission, tile planning, launch, polling).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "engine_passes.cuh"
+
+namespace pdlp {
+
+// ---- grid barrier (bounded) ----------------------------------------------------
+//
+// Arrive with a fenced atomic, wait for the generation to flip.  The wait is
+// bounded in wall time: on timeout the block records PDLP_ERR_BARRIER_TIMEOUT
+// in the control block and every block leaves the kernel at its next barrier.
+__device__ bool grid_barrier(Control* ctl, unsigned nblocks, long long timeout_ns, Smem& sm) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = &ctl->bar_gen;
+    volatile int* err = &ctl->error;
+    const unsigned g = *gen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(&ctl->bar_count, 1u) + 1u;
+    int ok = 1;
+    if (arrived == nblocks) {
+      atomicExch(&ctl->bar_count, 0u);
+      __threadfence();
+      atomicAdd((unsigned*)&ctl->bar_gen, 1u);
+    } else {
+      const long long t0 = global_ns();
+      unsigned spins = 0;
+      while (*gen == g) {
+        if ((++spins & 255u) == 0u) {
+          if (*err != 0) { ok = 0; break; }
+          if (global_ns() - t0 > timeout_ns) {
+            atomicCAS((int*)&ctl->error, 0, PDLP_ERR_BARRIER_TIMEOUT);
+            ok = 0;
+            break;
+          }
+        }
+      }
+    }
+    __threadfence();
+    sm.flag = ok && (*err == 0);
+  }
+  __syncthreads();
+  return sm.flag != 0;
+}
+
+__global__ void __launch_bounds__(kBlock) engine_persistent(EngineArgs A) {
+  __shared__ Smem sm;
+  const unsigned nb = gridDim.x;
+  const int b = blockIdx.x;
+  const int r0 = A.rblock[b], r1 = A.rblock[b + 1];
+  const int c0 = A.cblock[b], c1 = A.cblock[b + 1];
+  for (long long step = 0; step < A.max_steps; ++step) {
+    if (threadIdx.x == 0) sm.flag = *(volatile int*)&A.ctl->active;
+    __syncthreads();
+    if (sm.flag <= 0) return;
+    __syncthreads();
+    for (int t = r0; t < r1; ++t) process_rtile(A, t, sm);
+    if (!grid_barrier(A.ctl, nb, A.barrier_timeout_ns, sm)) return;
+    for (int t = c0; t < c1; ++t) process_ctile(A, t, sm);
+    if (!grid_barrier(A.ctl, nb, A.barrier_timeout_ns, sm)) return;
+  }
+}
+
+// One pass over all tiles of one side; kernel boundaries are the barriers.
+__global__ void __launch_bounds__(kBlock) engine_pass(EngineArgs A, int side) {
+  __shared__ Smem sm;
+  if (side == 0) {
+    for (int t = blockIdx.x; t < A.n_rtiles; t += gridDim.x) process_rtile(A, t, sm);
+  } else {
+    for (int t = blockIdx.x; t < A.n_ctiles; t += gridDim.x) process_ctile(A, t, sm);
+  }
+}
+
+// ---- admission kernels ----------------------------------------------------------
+
+// int64 compressed pointers -> int32, with structural checks.
+__global__ void convert_pointers(const long long* src, int* dst, int n, long long nnz, int* err) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > n) return;
+  long long v = src[i];
+  if (v < 0 || v > nnz || (i == 0 && v != 0) || (i == n && v != nnz) ||
+      (i < n && src[i + 1] < v))
+    atomicOr(err, 1);
+  dst[i] = (int)v;
+}
+
+__global__ void check_indices(const int* idx, long long nnz, int bound, int* err) {
+  long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; p < nnz; p += (long long)gridDim.x * blockDim.x) {
+    int v = idx[p];
+    if (v < 0 || v >= bound) atomicOr(err, 1);
+  }
+}
+
+__global__ void check_finite(const double* a, long long n, int allow_inf, int* err) {
+  long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; p < n; p += (long long)gridDim.x * blockDim.x) {
+    double v = a[p];
+    if (isnan(v) || (!allow_inf && isinf(v))) atomicOr(err, 2);
+  }
+}
+
+}  // namespace pdlp
+
+// ============================================================================
+// host runtime
+// ============================================================================
+
+namespace {
+
+using namespace pdlp;
+
+thread_local std::string g_err;
+
+constexpr size_t kAlign = 256;
+
+size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+
+int default_tile_rows() { return 512; }
+int default_tile_nnz() { return 8192; }
+int heavy_threshold() { return 4096; }
+
+int lanes_for(long long nnz, long long rows) {
+  if (rows <= 0) return 1;
+  double avg = (double)nnz / (double)rows;
+  int L = 1;
+  while (L < 32 && L < avg) L <<= 1;
+  return L;
+}
+
+// Split the rows of one side into tiles of at most `rows_cap` rows and about
+// `nnz_cap` entries; a row longer than the heavy threshold is a tile alone.
+void plan_tiles(const int64_t* ptr, int nrows, int inst, int rows_cap, int nnz_cap,
+                std::vector<Tile>& out, std::vector<double>& weight) {
+  const size_t first = out.size();
+  int b = 0;
+  long long acc = 0;
+  const int heavy = heavy_threshold();
+  for (int r = 0; r < nrows; ++r) {
+    long long len = ptr[r + 1] - ptr[r];
+    if (len > heavy) {
+      if (r > b) out.push_back({inst, b, r, 0});
+      out.push_back({inst, r, r + 1, 1});
+      b = r + 1;
+      acc = 0;
+      continue;
+    }
+    if (r > b && (r - b >= rows_cap || acc + len > nnz_cap)) {
+      out.push_back({inst, b, r, 0});
+      b = r;
+      acc = 0;
+    }
+    acc += len;
+  }
+  if (nrows > b) out.push_back({inst, b, nrows, 0});
+  if (nrows == 0) out.push_back({inst, 0, 0, 0});   // the pass still finishes
+  // work estimate per tile: entries (value + index + gather) and rows (vectors)
+  for (size_t i = first; i < out.size(); ++i) {
+    const Tile& t = out[i];
+    weight.push_back((double)(ptr[t.end] - ptr[t.begin]) * 3.0 + (t.end - t.begin) * 10.0 + 200.0);
+  }
+}
+
+struct Slot {
+  bool used = false;
+  bool running = false;
+  int m = 0, n = 0;
+  long long nnz = 0;
+  void* arena = nullptr;
+  size_t bytes = 0;
+  Inst inst{};
+  std::vector<Tile> rt, ct;   // tiles with local ranges (inst field = slot)
+  std::vector<double> rtw, ctw;   // work estimate per tile
+  double bytes_per_iter = 0.0;
+};
+
+}  // namespace
+
+struct pdlp_batch {
+  cudaStream_t stream = nullptr;
+  pdlp_batch_config cfg{};
+  std::vector<Slot> slots;
+  int n_running = 0;
+  size_t bytes_held = 0;
+  // device arrays
+  Inst* d_inst = nullptr;
+  State* d_state = nullptr;
+  unsigned* d_counters = nullptr;
+  Control* d_ctl = nullptr;
+  Tile* d_rtiles = nullptr;
+  Tile* d_ctiles = nullptr;
+  int* d_rblock = nullptr;
+  int* d_cblock = nullptr;
+  double* d_partials = nullptr;
+  size_t cap_rtiles = 0, cap_ctiles = 0, cap_blocks = 0, cap_partials = 0;
+  int n_rtiles = 0, n_ctiles = 0, grid = 0;
+  bool dirty = true;
+  bool broken = false;
+  // pinned host staging
+  Control* h_ctl = nullptr;
+  State* h_state = nullptr;
+  int sms = 0, coop_blocks_per_sm = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0.0, last_bytes = 0.0;
+  long long last_iters = 0;
+  std::vector<long long> iters_before;
+};
+
+namespace pdlp {
+
+void set_error(const std::string& msg) { g_err = msg; }
+const std::string& get_error() { return g_err; }
+
+}  // namespace pdlp
+
+namespace {
+
+int ensure_capacity(void** ptr, size_t* cap, size_t need, size_t elem) {
+  if (need <= *cap && *ptr) return PDLP_OK;
+  size_t n = std::max(need, (size_t)16);
+  n = std::max(n, *cap * 2);
+  if (*ptr) cudaFree(*ptr);
+  *ptr = nullptr;
+  cudaError_t e = cudaMalloc(ptr, n * elem);
+  if (e != cudaSuccess) { *cap = 0; return cuda_fail(e, "cudaMalloc(engine tables)"); }
+  *cap = n;
+  return PDLP_OK;
+}
+
+// Arena layout of one slot.
+struct Layout {
+  size_t off = 0;
+  size_t take(size_t bytes) { size_t o = off; off += align_up(bytes ? bytes : 1); return o; }
+};
+
+struct SlotLayout {
+  size_t rp32, cp32, ri, ci, rx0, cx0, rx, cx, kind, v0, tmp64;
+  size_t c0, rl0, ru0, lo0, hi0;
+  size_t mvec[14];   // c-side... see fill
+  size_t nvec[16];
+  size_t hist;
+  size_t total;
+};
+
+SlotLayout layout_for(int m, int n, long long nnz, bool kind, bool v0, int hist_cap) {
+  Layout L;
+  SlotLayout s{};
+  s.rp32 = L.take(sizeof(int) * (size_t)(m + 1));
+  s.cp32 = L.take(sizeof(int) * (size_t)(n + 1));
+  s.ri = L.take(sizeof(int) * (size_t)nnz);
+  s.ci = L.take(sizeof(int) * (size_t)nnz);
+  s.rx0 = L.take(sizeof(double) * (size_t)nnz);
+  s.cx0 = L.take(sizeof(double) * (size_t)nnz);
+  s.rx = L.take(sizeof(double) * (size_t)nnz);
+  s.cx = L.take(sizeof(double) * (size_t)nnz);
+  s.kind = kind ? L.take((size_t)n) : 0;
+  s.v0 = v0 ? L.take(sizeof(double) * (size_t)n) : 0;
+  s.tmp64 = L.take(sizeof(long long) * (size_t)(std::max(m, n) + 1));
+  s.c0 = L.take(sizeof(double) * (size_t)n);
+  s.lo0 = L.take(sizeof(double) * (size_t)n);
+  s.hi0 = L.take(sizeof(double) * (size_t)n);
+  s.rl0 = L.take(sizeof(double) * (size_t)m);
+  s.ru0 = L.take(sizeof(double) * (size_t)m);
+  for (int i = 0; i < 14; ++i) s.mvec[i] = L.take(sizeof(double) * (size_t)m);
+  for (int i = 0; i < 16; ++i) s.nvec[i] = L.take(sizeof(double) * (size_t)n);
+  s.hist = L.take(sizeof(double) * 5 * (size_t)std::max(hist_cap, 0));
+  s.total = L.off;
+  return s;
+}
+
+int copy_in(void* dst, const void* src, size_t bytes, int memory, cudaStream_t st) {
+  if (bytes == 0) return PDLP_OK;
+  if (!src) return fail(PDLP_ERR_ARG, "a required input array is NULL");
+  PDLP_CUDA(cudaMemcpyAsync(dst, src, bytes,
+                            memory == PDLP_MEM_HOST ? cudaMemcpyHostToDevice
+                                                    : cudaMemcpyDeviceToDevice, st));
+  return PDLP_OK;
+}
+
+// Contiguous chunks of the tile list with about equal work, one per block.
+void block_ranges(const std::vector<double>& w, int G, std::vector<int>& out) {
+  const size_t T = w.size();
+  double total = 0.0;
+  for (size_t i = 0; i < T; ++i) total += w[i];
+  out.assign(G + 1, (int)T);
+  out[0] = 0;
+  double acc = 0.0;
+  int b = 1;
+  for (size_t i = 0; i < T && b < G; ++i) {
+    acc += w[i];
+    while (b < G && acc >= total * b / G) { out[b] = (int)i + 1; ++b; }
+  }
+  for (; b < G; ++b) out[b] = (int)T;
+  out[G] = (int)T;
+}
+
+}  // namespace
+
+static int rebuild(pdlp_batch* b) {
+  std::vector<Tile> rt, ct;
+  std::vector<double> rw, cw;
+  for (size_t s = 0; s < b->slots.size(); ++s) {
+    Slot& sl = b->slots[s];
+    if (!sl.used || !sl.running) continue;
+    sl.inst.rt_begin = (int)rt.size();
+    rt.insert(rt.end(), sl.rt.begin(), sl.rt.end());
+    rw.insert(rw.end(), sl.rtw.begin(), sl.rtw.end());
+    sl.inst.rt_end = (int)rt.size();
+    sl.inst.ct_begin = (int)ct.size();
+    ct.insert(ct.end(), sl.ct.begin(), sl.ct.end());
+    cw.insert(cw.end(), sl.ctw.begin(), sl.ctw.end());
+    sl.inst.ct_end = (int)ct.size();
+  }
+  b->n_rtiles = (int)rt.size();
+  b->n_ctiles = (int)ct.size();
+  int G = std::max(1, std::min(b->sms * b->coop_blocks_per_sm,
+                               std::max(b->n_rtiles, b->n_ctiles)));
+  b->grid = G;
+  std::vector<int> rb, cb;
+  block_ranges(rw, G, rb);
+  block_ranges(cw, G, cb);
+  int rc;
+  if ((rc = ensure_capacity((void**)&b->d_rtiles, &b->cap_rtiles, rt.size(), sizeof(Tile)))) return rc;
+  if ((rc = ensure_capacity((void**)&b->d_ctiles, &b->cap_ctiles, ct.size(), sizeof(Tile)))) return rc;
+  size_t need_blocks = (size_t)G + 1;
+  if (need_blocks > b->cap_blocks || !b->d_rblock) {
+    size_t cap = b->cap_blocks;
+    if ((rc = ensure_capacity((void**)&b->d_rblock, &cap, need_blocks, sizeof(int)))) return rc;
+    cap = b->cap_blocks;
+    if ((rc = ensure_capacity((void**)&b->d_cblock, &cap, need_blocks, sizeof(int)))) return rc;
+    b->cap_blocks = cap;
+  }
+  if ((rc = ensure_capacity((void**)&b->d_partials, &b->cap_partials,
+                            (rt.size() + ct.size()) * kNP, sizeof(double)))) return rc;
+  cudaStream_t st = b->stream;
+  if (!rt.empty()) PDLP_CUDA(cudaMemcpyAsync(b->d_rtiles, rt.data(), rt.size() * sizeof(Tile), cudaMemcpyHostToDevice, st));
+  if (!ct.empty()) PDLP_CUDA(cudaMemcpyAsync(b->d_ctiles, ct.data(), ct.size() * sizeof(Tile), cudaMemcpyHostToDevice, st));
+  PDLP_CUDA(cudaMemcpyAsync(b->d_rblock, rb.data(), rb.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  PDLP_CUDA(cudaMemcpyAsync(b->d_cblock, cb.data(), cb.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  std::vector<Inst> insts(b->slots.size());
+  for (size_t s = 0; s < b->slots.size(); ++s) insts[s] = b->slots[s].inst;
+  PDLP_CUDA(cudaMemcpyAsync(b->d_inst, insts.data(), insts.size() * sizeof(Inst), cudaMemcpyHostToDevice, st));
+  // the staging vectors die at return: wait for the copies
+  PDLP_CUDA(cudaStreamSynchronize(st));
+  b->dirty = false;
+  return PDLP_OK;
+}
+
+extern "C" {
+
+int pdlp_abi_version(void) { return PDLP_ABI_VERSION; }
+
+const char* pdlp_last_error(void) { return g_err.c_str(); }
+
+void pdlp_params_default(pdlp_params* p) {
+  std::memset(p, 0, sizeof(*p));
+  p->eps_abs = 1e-8;
+  p->eps_rel = 1e-8;
+  p->feas_cap = 1e-6;
+  p->max_iter = 200000;
+  p->time_limit = 600.0;
+  p->check_every = 64;
+  p->stepsize_every = 8;
+  p->beta_sufficient = 0.2;
+  p->beta_necessary = 0.8;
+  p->beta_artificial = 0.36;
+  p->primal_weight_smoothing = 0.5;
+  p->scaling = PDLP_SCALING_PDLP;
+  p->power_start = nullptr;
+  p->time_used = 0.0;
+  p->history_capacity = 0;
+}
+
+void pdlp_batch_config_default(pdlp_batch_config* c) {
+  std::memset(c, 0, sizeof(*c));
+  c->max_slots = 1;
+  c->persistent = 1;
+  c->block_threads = kBlock;
+  c->tile_rows = default_tile_rows();
+  c->tile_nnz = default_tile_nnz();
+  c->lanes_override = 0;
+  c->memory_budget = 0;
+}
+
+int64_t pdlp_slot_bytes(int32_t m, int32_t n, int64_t nnz) {
+  return (int64_t)layout_for(m, n, nnz, true, true, 4096).total;
+}
+
+int pdlp_batch_create(const pdlp_batch_config* cfg, void* stream, pdlp_batch** out) {
+  if (!out) return fail(PDLP_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  pdlp_batch_config c;
+  pdlp_batch_config_default(&c);
+  if (cfg) c = *cfg;
+  if (c.max_slots <= 0) return fail(PDLP_ERR_ARG, "max_slots must be positive");
+  if (c.block_threads == 0) c.block_threads = kBlock;
+  if (c.block_threads != kBlock) return fail(PDLP_ERR_ARG, "block_threads must be 256");
+  if (c.tile_rows <= 0) c.tile_rows = default_tile_rows();
+  if (c.tile_rows > kMaxTileRows) return fail(PDLP_ERR_ARG, "tile_rows exceeds 1024");
+  if (c.tile_nnz <= 0) c.tile_nnz = default_tile_nnz();
+  if (c.lanes_override && (c.lanes_override & (c.lanes_override - 1)))
+    return fail(PDLP_ERR_ARG, "lanes_override must be a power of two");
+  pdlp_batch* b = new pdlp_batch();
+  b->stream = (cudaStream_t)stream;
+  b->cfg = c;
+  b->slots.resize(c.max_slots);
+  b->iters_before.assign(c.max_slots, 0);
+  int dev = 0;
+  cudaError_t e;
+  auto bail = [&](cudaError_t err, const char* what) {
+    pdlp_batch_destroy(b);
+    return cuda_fail(err, what);
+  };
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return bail(e, "cudaGetDevice");
+  if ((e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+    return bail(e, "cudaDeviceGetAttribute");
+  int coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->coop_blocks_per_sm, engine_persistent,
+                                                          kBlock, 0)) != cudaSuccess)
+    return bail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (!coop || b->coop_blocks_per_sm < 1) b->cfg.persistent = 0;
+  if ((e = cudaMalloc(&b->d_inst, sizeof(Inst) * c.max_slots)) != cudaSuccess) return bail(e, "cudaMalloc");
+  if ((e = cudaMalloc(&b->d_state, sizeof(State) * c.max_slots)) != cudaSuccess) return bail(e, "cudaMalloc");
+  if ((e = cudaMalloc(&b->d_counters, sizeof(unsigned) * 2 * c.max_slots)) != cudaSuccess) return bail(e, "cudaMalloc");
+  if ((e = cudaMalloc(&b->d_ctl, sizeof(Control))) != cudaSuccess) return bail(e, "cudaMalloc");
+  if ((e = cudaMallocHost(&b->h_ctl, sizeof(Control))) != cudaSuccess) return bail(e, "cudaMallocHost");
+  if ((e = cudaMallocHost(&b->h_state, sizeof(State) * c.max_slots)) != cudaSuccess) return bail(e, "cudaMallocHost");
+  cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2 * c.max_slots, b->stream);
+  cudaMemsetAsync(b->d_ctl, 0, sizeof(Control), b->stream);
+  cudaMemsetAsync(b->d_state, 0, sizeof(State) * c.max_slots, b->stream);
+  std::vector<Inst> zero(c.max_slots);
+  std::memset(zero.data(), 0, sizeof(Inst) * zero.size());
+  cudaMemcpyAsync(b->d_inst, zero.data(), sizeof(Inst) * zero.size(), cudaMemcpyHostToDevice, b->stream);
+  cudaEventCreate(&b->ev0);
+  cudaEventCreate(&b->ev1);
+  if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return bail(e, "cudaStreamSynchronize");
+  *out = b;
+  return PDLP_OK;
+}
+
+int pdlp_batch_destroy(pdlp_batch* b) {
+  if (!b) return PDLP_OK;
+  cudaStreamSynchronize(b->stream);
+  for (auto& s : b->slots) if (s.arena) cudaFree(s.arena);
+  cudaFree(b->d_inst); cudaFree(b->d_state); cudaFree(b->d_counters); cudaFree(b->d_ctl);
+  cudaFree(b->d_rtiles); cudaFree(b->d_ctiles); cudaFree(b->d_rblock); cudaFree(b->d_cblock);
+  cudaFree(b->d_partials);
+  if (b->h_ctl) cudaFreeHost(b->h_ctl);
+  if (b->h_state) cudaFreeHost(b->h_state);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  delete b;
+  return PDLP_OK;
+}
+
+int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_params* params,
+                     int32_t* slot_out) {
+  if (!b || !P) return fail(PDLP_ERR_ARG, "NULL batch or problem");
+  if (b->broken) return fail(PDLP_ERR_STATE, "batch is unusable after a device wait timed out");
+  pdlp_params prm;
+  pdlp_params_default(&prm);
+  if (params) prm = *params;
+  const int m = P->m, n = P->n;
+  const long long nnz = P->nnz;
+  if (m < 0 || n < 0 || nnz < 0) return fail(PDLP_ERR_ARG, "negative dimension");
+  if (nnz > 0x7fffffffLL) return fail(PDLP_ERR_ARG, "nnz must fit in int32");
+  if (P->sense != 1 && P->sense != -1) return fail(PDLP_ERR_ARG, "sense must be 1 or -1");
+  if (P->memory != PDLP_MEM_HOST && P->memory != PDLP_MEM_DEVICE)
+    return fail(PDLP_ERR_ARG, "memory must be PDLP_MEM_HOST or PDLP_MEM_DEVICE");
+  if (prm.check_every <= 0 || prm.stepsize_every <= 0) return fail(PDLP_ERR_ARG, "check_every and stepsize_every must be positive");
+  if (prm.max_iter < 0) return fail(PDLP_ERR_ARG, "max_iter must be >= 0");
+  if (prm.scaling < 0 || prm.scaling > 3) return fail(PDLP_ERR_ARG, "unknown scaling method");
+  if (!std::isfinite(P->obj_offset)) return fail(PDLP_ERR_NUMERICAL, "obj_offset is not finite");
+  int slot = -1;
+  for (size_t s = 0; s < b->slots.size(); ++s) if (!b->slots[s].used) { slot = (int)s; break; }
+  if (slot < 0) return fail(PDLP_ERR_STATE, "no free slot");
+  cudaStream_t st = b->stream;
+
+  // host copies of the pointer arrays: validation and tile planning
+  std::vector<int64_t> hrp, hcp;
+  const int64_t* rp = P->rp;
+  const int64_t* cp = P->cp;
+  if (!rp || !cp) return fail(PDLP_ERR_ARG, "rp/cp are NULL");
+  if (P->memory == PDLP_MEM_DEVICE) {
+    hrp.resize(m + 1); hcp.resize(n + 1);
+    PDLP_CUDA(cudaMemcpyAsync(hrp.data(), rp, sizeof(int64_t) * (m + 1), cudaMemcpyDeviceToHost, st));
+    PDLP_CUDA(cudaMemcpyAsync(hcp.data(), cp, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, st));
+    PDLP_CUDA(cudaStreamSynchronize(st));
+    rp = hrp.data(); cp = hcp.data();
+  }
+  auto check_ptr = [&](const int64_t* p, int len) {
+    if (p[0] != 0 || p[len] != nnz) return false;
+    for (int i = 0; i < len; ++i) if (p[i + 1] < p[i]) return false;
+    return true;
+  };
+  if (!check_ptr(rp, m) || !check_ptr(cp, n))
+    return fail(PDLP_ERR_ARG, "malformed compressed pointers (must start at 0, be non-decreasing and end at nnz)");
+
+  const int hist_cap = std::max(0, prm.history_capacity);
+  const bool has_kind = P->kind != nullptr;
+  const bool has_v0 = prm.power_start != nullptr;
+  SlotLayout L = layout_for(m, n, nnz, has_kind, has_v0, hist_cap);
+  size_t budget = (size_t)b->cfg.memory_budget;
+  if (budget == 0) {
+    size_t fr = 0, tot = 0;
+    PDLP_CUDA(cudaMemGetInfo(&fr, &tot));
+    budget = b->bytes_held + (fr > ((size_t)1 << 30) ? fr - ((size_t)1 << 30) : 0);
+  }
+  if (b->bytes_held + L.total > budget)
+    return fail(PDLP_ERR_OOM, "admission refused: the LP does not fit the memory budget");
+  void* arena = nullptr;
+  cudaError_t e = cudaMalloc(&arena, L.total);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(PDLP_ERR_OOM, std::string("admission refused: cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  char* base = (char*)arena;
+  auto at = [&](size_t off) { return (void*)(base + off); };
+  int rc = PDLP_OK;
+  auto cleanup = [&](int code) { cudaStreamSynchronize(st); cudaFree(arena); return code; };
+
+  const int mem = P->memory;
+  // pointers: copy int64 into scratch, convert to int32 with checks
+  State init{};
+  std::memset(&init, 0, sizeof(init));
+  // the state's error word doubles as the validation flag
+  int* err_flag = &b->d_state[slot].error;
+  PDLP_CUDA(cudaMemsetAsync(&b->d_state[slot], 0, sizeof(State), st));
+  if ((rc = copy_in(at(L.tmp64), P->rp, sizeof(int64_t) * (m + 1), mem, st))) return cleanup(rc);
+  convert_pointers<<<(m + 256) / 256, 256, 0, st>>>((const long long*)at(L.tmp64), (int*)at(L.rp32), m, nnz, err_flag);
+  if ((rc = copy_in(at(L.tmp64), P->cp, sizeof(int64_t) * (n + 1), mem, st))) return cleanup(rc);
+  convert_pointers<<<(n + 256) / 256, 256, 0, st>>>((const long long*)at(L.tmp64), (int*)at(L.cp32), n, nnz, err_flag);
+  if ((rc = copy_in(at(L.ri), P->ri, sizeof(int) * nnz, mem, st))) return cleanup(rc);
+  if ((rc = copy_in(at(L.ci), P->ci, sizeof(int) * nnz, mem, st))) return cleanup(rc);
+  if ((rc = copy_in(at(L.rx0), P->rx, sizeof(double) * nnz, mem, st))) return cleanup(rc);
+  if ((rc = copy_in(at(L.cx0), P->cx, sizeof(double) * nnz, mem, st))) return cleanup(rc);
+  if ((rc = copy_in(at(L.c0), P->c, sizeof(double) * n, mem, st))) return cleanup(rc);
+  if ((rc = copy_in(at(L.lo0), P->col_lb, sizeof(double) * n, mem, st))) return cleanup(rc);
+  if ((rc = copy_in(at(L.hi0), P->col_ub, sizeof(double) * n, mem, st))) return cleanup(rc);
+  if ((rc = copy_in(at(L.rl0), P->row_lb, sizeof(double) * m, mem, st))) return cleanup(rc);
+  if ((rc = copy_in(at(L.ru0), P->row_ub, sizeof(double) * m, mem, st))) return cleanup(rc);
+  if (has_kind && (rc = copy_in(at(L.kind), P->kind, (size_t)n, mem, st))) return cleanup(rc);
+  if (has_v0 && (rc = copy_in(at(L.v0), prm.power_start, sizeof(double) * n, mem, st))) return cleanup(rc);
+  auto grid_for = [](long long cnt) { return (int)std::max(1LL, std::min(4096LL, (cnt + 255) / 256)); };
+  if (nnz > 0) {
+    check_indices<<<grid_for(nnz), 256, 0, st>>>((const int*)at(L.ri), nnz, n, err_flag);
+    check_indices<<<grid_for(nnz), 256, 0, st>>>((const int*)at(L.ci), nnz, m, err_flag);
+    check_finite<<<grid_for(nnz), 256, 0, st>>>((const double*)at(L.rx0), nnz, 0, err_flag);
+    check_finite<<<grid_for(nnz), 256, 0, st>>>((const double*)at(L.cx0), nnz, 0, err_flag);
+  }
+  if (n > 0) {
+    check_finite<<<grid_for(n), 256, 0, st>>>((const double*)at(L.c0), n, 0, err_flag);
+    check_finite<<<grid_for(n), 256, 0, st>>>((const double*)at(L.lo0), n, 1, err_flag);
+    check_finite<<<grid_for(n), 256, 0, st>>>((const double*)at(L.hi0), n, 1, err_flag);
+  }
+  if (m > 0) {
+    check_finite<<<grid_for(m), 256, 0, st>>>((const double*)at(L.rl0), m, 1, err_flag);
+    check_finite<<<grid_for(m), 256, 0, st>>>((const double*)at(L.ru0), m, 1, err_flag);
+  }
+  int herr = 0;
+  PDLP_CUDA(cudaMemcpyAsync(&herr, err_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) { cudaFree(arena); return cuda_fail(e, "admission copies"); }
+  if (herr & 1) { cudaFree(arena); return fail(PDLP_ERR_ARG, "malformed sparse structure (pointer or index out of range)"); }
+  if (herr & 2) { cudaFree(arena); return fail(PDLP_ERR_NUMERICAL, "NaN in the data, or an infinite matrix entry or cost"); }
+
+  Slot& S = b->slots[slot];
+  S = Slot();
+  S.used = true;
+  S.running = true;
+  S.m = m; S.n = n; S.nnz = nnz;
+  S.arena = arena;
+  S.bytes = L.total;
+  Inst& I = S.inst;
+  std::memset(&I, 0, sizeof(I));
+  I.m = m; I.n = n; I.nnz = nnz;
+  I.lanes_r = b->cfg.lanes_override ? b->cfg.lanes_override : lanes_for(nnz, m);
+  I.lanes_c = b->cfg.lanes_override ? b->cfg.lanes_override : lanes_for(nnz, n);
+  I.sense = P->sense;
+  I.ruiz_iters = prm.scaling == PDLP_SCALING_PDLP ? 10 : (prm.scaling == PDLP_SCALING_RUIZ ? 20 : 0);
+  I.use_pc = prm.scaling == PDLP_SCALING_PDLP || prm.scaling == PDLP_SCALING_POCK_CHAMBOLLE;
+  I.scale_none = prm.scaling == PDLP_SCALING_NONE;
+  I.rp = (const int*)at(L.rp32); I.ri = (const int*)at(L.ri);
+  I.cp = (const int*)at(L.cp32); I.ci = (const int*)at(L.ci);
+  I.rx0 = (const double*)at(L.rx0); I.cx0 = (const double*)at(L.cx0);
+  I.rx = (double*)at(L.rx); I.cx = (double*)at(L.cx);
+  I.c0 = (const double*)at(L.c0); I.rl0 = (const double*)at(L.rl0); I.ru0 = (const double*)at(L.ru0);
+  I.lo0 = (const double*)at(L.lo0); I.hi0 = (const double*)at(L.hi0);
+  I.kind = has_kind ? (const unsigned char*)at(L.kind) : nullptr;
+  I.offset0 = P->obj_offset;
+  double** mv[14] = {&I.rl, &I.ru, &I.rs, &I.y, &I.ax, &I.dy, &I.ynew, &I.adx, &I.sumy,
+                     &I.ybar, &I.axbar, &I.axf, &I.yrst, &I.yout};
+  for (int i = 0; i < 14; ++i) *mv[i] = (double*)at(L.mvec[i]);
+  double** nv[16] = {&I.c, &I.lo, &I.hi, &I.cs, &I.x, &I.aty, &I.dx, &I.xnew, &I.sumx,
+                     &I.xbar, &I.atybar, &I.atyf, &I.xrst, &I.xout, &I.dout, nullptr};
+  for (int i = 0; i < 15; ++i) *nv[i] = (double*)at(L.nvec[i]);
+  I.v0 = has_v0 ? (const double*)at(L.v0) : nullptr;
+  I.hist = hist_cap ? (double*)at(L.hist) : nullptr;
+  I.hist_cap = hist_cap;
+  I.eps_abs = prm.eps_abs; I.eps_rel = prm.eps_rel; I.feas_cap = prm.feas_cap;
+  I.max_iter = prm.max_iter;
+  I.time_limit_ns = prm.time_limit * 1e9;
+  I.time_used_ns = prm.time_used * 1e9;
+  I.check_every = prm.check_every; I.stepsize_every = prm.stepsize_every;
+  I.beta_s = prm.beta_sufficient; I.beta_n = prm.beta_necessary; I.beta_a = prm.beta_artificial;
+  I.theta = prm.primal_weight_smoothing;
+  plan_tiles(rp, m, slot, b->cfg.tile_rows, b->cfg.tile_nnz, S.rt, S.rtw);
+  plan_tiles(cp, n, slot, b->cfg.tile_rows, b->cfg.tile_nnz, S.ct, S.ctw);
+  S.bytes_per_iter = 24.0 * (double)nnz + 4.0 * (m + 1) + 4.0 * (n + 1) + 8.0 * (10.0 * m + 11.0 * n);
+
+  init.status = PDLP_STATUS_RUNNING;
+  init.final_status = PDLP_STATUS_RUNNING;
+  if (I.ruiz_iters > 0) { init.rmode = R_RUIZ; init.cmode = C_RUIZ; }
+  else { init.rmode = R_PC; init.cmode = C_PC; }
+  init.eta = 1.0; init.omega = 1.0; init.s_obj = 1.0;
+  PDLP_CUDA(cudaMemcpyAsync(&b->d_state[slot], &init, sizeof(State), cudaMemcpyHostToDevice, st));
+  PDLP_CUDA(cudaMemsetAsync(b->d_counters + 2 * slot, 0, 2 * sizeof(unsigned), st));
+  PDLP_CUDA(cudaStreamSynchronize(st));
+  b->bytes_held += L.total;
+  b->n_running += 1;
+  b->iters_before[slot] = 0;
+  b->dirty = true;
+  if (slot_out) *slot_out = slot;
+  return PDLP_OK;
+}
+
+int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out) {
+  if (!b) return fail(PDLP_ERR_ARG, "NULL batch");
+  if (b->broken) return fail(PDLP_ERR_STATE, "batch is unusable after a device wait timed out");
+  b->last_ms = 0.0; b->last_bytes = 0.0; b->last_iters = 0;
+  if (b->n_running == 0) { if (active_out) *active_out = 0; return PDLP_OK; }
+  int rc;
+  if (b->dirty && (rc = rebuild(b))) return rc;
+  cudaStream_t st = b->stream;
+  EngineArgs A{};
+  A.inst = b->d_inst; A.st = b->d_state;
+  A.rtiles = b->d_rtiles; A.n_rtiles = b->n_rtiles;
+  A.ctiles = b->d_ctiles; A.n_ctiles = b->n_ctiles;
+  A.rblock = b->d_rblock; A.cblock = b->d_cblock;
+  A.partials = b->d_partials; A.counters = b->d_counters; A.ctl = b->d_ctl;
+  A.max_steps = max_steps;
+  A.barrier_timeout_ns = 4000000000LL;
+  A.n_inst = (int)b->slots.size();
+  b->h_ctl->bar_count = 0; b->h_ctl->bar_gen = 0; b->h_ctl->active = b->n_running;
+  b->h_ctl->error = 0; b->h_ctl->error_where = 0;
+  PDLP_CUDA(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(Control), cudaMemcpyHostToDevice, st));
+  PDLP_CUDA(cudaEventRecord(b->ev0, st));
+  if (b->cfg.persistent) {
+    void* args[] = {&A};
+    PDLP_CUDA(cudaLaunchCooperativeKernel((void*)engine_persistent, dim3(b->grid), dim3(kBlock),
+                                          args, 0, st));
+  } else {
+    // one launch per pass, in chunks; the engine is idle once every LP is done
+    const int g_r = std::max(1, std::min(b->n_rtiles, b->sms * 8));
+    const int g_c = std::max(1, std::min(b->n_ctiles, b->sms * 8));
+    const int64_t chunk = 64;
+    for (int64_t done = 0; done < max_steps; done += chunk) {
+      const int64_t k = std::min(chunk, max_steps - done);
+      for (int64_t s = 0; s < k; ++s) {
+        engine_pass<<<g_r, kBlock, 0, st>>>(A, 0);
+        engine_pass<<<g_c, kBlock, 0, st>>>(A, 1);
+      }
+      PDLP_CUDA(cudaGetLastError());
+      PDLP_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, st));
+      PDLP_CUDA(cudaStreamSynchronize(st));
+      if (b->h_ctl->active <= 0) break;
+    }
+  }
+  PDLP_CUDA(cudaEventRecord(b->ev1, st));
+  PDLP_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, st));
+  PDLP_CUDA(cudaMemcpyAsync(b->h_state, b->d_state, sizeof(State) * b->slots.size(), cudaMemcpyDeviceToHost, st));
+  PDLP_CUDA(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+  b->last_ms = ms;
+  if (b->h_ctl->error) {
+    b->broken = true;
+    return fail(b->h_ctl->error, "engine: a bounded grid barrier timed out; the batch was stopped");
+  }
+  int running = 0;
+  for (size_t s = 0; s < b->slots.size(); ++s) {
+    Slot& sl = b->slots[s];
+    if (!sl.used || !sl.running) continue;
+    const State& hs = b->h_state[s];
+    long long d = hs.iters_done - b->iters_before[s];
+    b->iters_before[s] = hs.iters_done;
+    b->last_iters += d;
+    b->last_bytes += d * sl.bytes_per_iter;
+    if (hs.status != PDLP_STATUS_RUNNING) { sl.running = false; b->dirty = true; }
+    else ++running;
+  }
+  b->n_running = running;
+  if (active_out) *active_out = running;
+  return PDLP_OK;
+}
+
+int pdlp_batch_last_timing(pdlp_batch* b, double* ms, double* iter_bytes, int64_t* iterations) {
+  if (!b) return fail(PDLP_ERR_ARG, "NULL batch");
+  if (ms) *ms = b->last_ms;
+  if (iter_bytes) *iter_bytes = b->last_bytes;
+  if (iterations) *iterations = b->last_iters;
+  return PDLP_OK;
+}
+
+int pdlp_batch_poll(pdlp_batch* b, int32_t slot, pdlp_result* r) {
+  if (!b || !r) return fail(PDLP_ERR_ARG, "NULL argument");
+  if (slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
+    return fail(PDLP_ERR_ARG, "no such slot");
+  State hs;
+  PDLP_CUDA(cudaMemcpyAsync(&hs, &b->d_state[slot], sizeof(State), cudaMemcpyDeviceToHost, b->stream));
+  PDLP_CUDA(cudaStreamSynchronize(b->stream));
+  std::memset(r, 0, sizeof(*r));
+  const double nan = std::nan("");
+  r->status = hs.status;
+  r->iterations = hs.k;
+  r->restarts = hs.restarts;
+  r->rejected_steps = hs.rejected;
+  const bool opt = hs.status == PDLP_STATUS_OPTIMAL;
+  r->primal_res = opt ? hs.fin[0] : nan;
+  r->dual_res = opt ? hs.fin[1] : nan;
+  r->gap = opt ? hs.fin[2] : nan;
+  r->primal_obj = opt ? hs.fin[3] : nan;
+  r->dual_obj = opt ? hs.fin[4] : nan;
+  r->step_size = hs.eta;
+  r->primal_weight = hs.omega;
+  r->objective = hs.status == PDLP_STATUS_RUNNING ? nan : hs.objective;
+  r->scale_obj = hs.s_obj;
+  r->history_len = hs.hist_len;
+  r->device_seconds = hs.t_end_ns > hs.t_start_ns ? (hs.t_end_ns - hs.t_start_ns) * 1e-9 : 0.0;
+  return PDLP_OK;
+}
+
+int pdlp_batch_fetch(pdlp_batch* b, int32_t slot, double* x, double* y, double* d,
+                     double* history, int32_t memory) {
+  if (!b) return fail(PDLP_ERR_ARG, "NULL batch");
+  if (slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
+    return fail(PDLP_ERR_ARG, "no such slot");
+  Slot& s = b->slots[slot];
+  if (s.running) return fail(PDLP_ERR_STATE, "slot is still running");
+  cudaMemcpyKind k = memory == PDLP_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  cudaStream_t st = b->stream;
+  if (x && s.n) PDLP_CUDA(cudaMemcpyAsync(x, s.inst.xout, sizeof(double) * s.n, k, st));
+  if (y && s.m) PDLP_CUDA(cudaMemcpyAsync(y, s.inst.yout, sizeof(double) * s.m, k, st));
+  if (d && s.n) PDLP_CUDA(cudaMemcpyAsync(d, s.inst.dout, sizeof(double) * s.n, k, st));
+  if (history && s.inst.hist_cap) {
+    State hs;
+    PDLP_CUDA(cudaMemcpyAsync(&hs, &b->d_state[slot], sizeof(State), cudaMemcpyDeviceToHost, st));
+    PDLP_CUDA(cudaStreamSynchronize(st));
+    if (hs.hist_len) PDLP_CUDA(cudaMemcpyAsync(history, s.inst.hist, sizeof(double) * 5 * hs.hist_len, k, st));
+  }
+  PDLP_CUDA(cudaStreamSynchronize(st));
+  return PDLP_OK;
+}
+
+int pdlp_batch_retire(pdlp_batch* b, int32_t slot) {
+  if (!b) return fail(PDLP_ERR_ARG, "NULL batch");
+  if (slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
+    return fail(PDLP_ERR_ARG, "no such slot");
+  Slot& s = b->slots[slot];
+  PDLP_CUDA(cudaStreamSynchronize(b->stream));
+  if (s.running) { b->n_running -= 1; }
+  cudaFree(s.arena);
+  b->bytes_held -= s.bytes;
+  s = Slot();
+  b->dirty = true;
+  return PDLP_OK;
+}
+
+int pdlp_batch_cancel(pdlp_batch* b, int32_t slot) {
+  if (!b) return fail(PDLP_ERR_ARG, "NULL batch");
+  if (slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
+    return fail(PDLP_ERR_ARG, "no such slot");
+  int one = 1;
+  PDLP_CUDA(cudaMemcpyAsync(&b->d_state[slot].cancel, &one, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  PDLP_CUDA(cudaStreamSynchronize(b->stream));
+  return PDLP_OK;
+}
+
+int pdlp_solve(const pdlp_problem_desc* prob, const pdlp_params* params, void* stream,
+               pdlp_result* result, double* x, double* y, double* d, double* history,
+               int32_t out_memory) {
+  pdlp_batch_config cfg;
+  pdlp_batch_config_default(&cfg);
+  cfg.max_slots = 1;
+  pdlp_batch* b = nullptr;
+  int rc = pdlp_batch_create(&cfg, stream, &b);
+  if (rc) return rc;
+  int slot = -1;
+  if ((rc = pdlp_batch_admit(b, prob, params, &slot))) { pdlp_batch_destroy(b); return rc; }
+  int active = 1;
+  while (active > 0) {
+    if ((rc = pdlp_batch_step(b, 1 << 20, &active))) { pdlp_batch_destroy(b); return rc; }
+  }
+  pdlp_result r;
+  if ((rc = pdlp_batch_poll(b, slot, &r))) { pdlp_batch_destroy(b); return rc; }
+  if (result) *result = r;
+  if ((rc = pdlp_batch_fetch(b, slot, x, y, d, history, out_memory))) { pdlp_batch_destroy(b); return rc; }
+  pdlp_batch_destroy(b);
+  return PDLP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,70 @@
+"""The C-ABI library loads and exports every entry point the header declares
+(no compute: these run without a GPU)."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from sovereign_moe_b200 import _lib
+from sovereign_moe_b200.pdlp import PDLPParams
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    text = open(os.path.join(ROOT, "include", "pdlp_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pdlp_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_bound_surface():
+    names = declared_functions()
+    assert names, "no declarations parsed"
+    assert set(names) == set(_lib.SIGNATURES), set(names) ^ set(_lib.SIGNATURES)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+
+
+def test_abi_version_and_defaults_match_reference_params():
+    lib = _lib.load()
+    assert lib.pdlp_abi_version() == 1
+    p = _lib.Params()
+    lib.pdlp_params_default(ctypes.byref(p))
+    ref = PDLPParams()
+    for f in ("eps_abs", "eps_rel", "feas_cap", "max_iter", "time_limit", "check_every",
+              "stepsize_every", "beta_sufficient", "beta_necessary", "beta_artificial",
+              "primal_weight_smoothing"):
+        assert getattr(p, f) == getattr(ref, f), f
+    assert p.scaling == _lib.SCALING["pdlp"]
+
+
+def test_struct_layouts_match_the_header():
+    # sizes of the C structs on x86-64 (natural alignment)
+    assert ctypes.sizeof(_lib.ProblemDesc) == 4 + 4 + 8 + 12 * 8 + 8 + 4 + 4
+    assert ctypes.sizeof(_lib.BatchConfig) == 6 * 4 + 8
+    assert ctypes.sizeof(_lib.Result) == 8 + 3 * 8 + 9 * 8 + 8 + 8
+
+
+def test_slot_bytes_grows_with_the_problem():
+    lib = _lib.load()
+    small = lib.pdlp_slot_bytes(100, 300, 1200)
+    big = lib.pdlp_slot_bytes(1000, 3000, 12000)
+    assert 0 < small < big
+    # about 90 bytes per nonzero plus vectors, like the reference's own estimate
+    assert big < 200 * 12000 + 400 * 4000
+
+
+def test_cpu_device_is_refused():
+    from sovereign_moe_b200 import solve_pdlp
+    from sovereign_moe_b200.workloads import single_small
+    with pytest.raises(ValueError):
+        solve_pdlp(single_small(0).problem, PDLPParams(device="cpu"))
+    with pytest.raises(ValueError):
+        solve_pdlp(single_small(0).problem, PDLPParams(device="tpu"))

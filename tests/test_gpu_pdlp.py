@@ -1,0 +1,174 @@
+"""End-to-end parity of the B200 engine with the reference PDLP.
+
+Each golden case (tests/golden/, outputs of the reference solve_pdlp) is
+solved through the C ABI and compared:
+
+* status equal to the reference's;
+* OPTIMAL: objective within 1e-6 relative of the reference's (and of the
+  known optimum where the LP was built around one), and the point accepted by
+  the independent verifier (oracle/verify_oracle.py, bench/verify.py) at
+  feas_tol 1e-6 -- the reference's "OPTIMAL => verifier accepts"
+  (tests/test_solvers.py:102-118);
+* iteration counts close to the reference's: the engine runs the same
+  iteration in float64 but sums in a different (fixed, tree) order, so the
+  trajectories agree to rounding, and a restart decision can flip late;
+* a 100-iteration run stopped by max_iter lands on the reference's iterate to
+  1e-8: the whole pipeline (scaling, power iteration, line search, restarts)
+  follows the reference step by step.
+"""
+
+import numpy as np
+import pytest
+
+import golden_cases as gc
+from oracle import verify_oracle as vo
+from sovereign_moe_b200.pdlp import PDLPParams, solve_pdlp
+from sovereign_moe_b200.problem import Status
+
+pytestmark = pytest.mark.gpu
+
+OPTIMAL_CASES = ["toy", "testprob", "toy_min", "badly_scaled_s1", "badly_scaled_s2",
+                 "badly_scaled_s3", "dual_regression", "agree", "small_known_s0",
+                 "small_known_s1"]
+
+
+def _params(name):
+    return PDLPParams(device="gpu", **gc.PARAMS[name])
+
+
+@pytest.mark.parametrize("name", OPTIMAL_CASES)
+def test_optimal_cases_match_reference(require_gpu, name):
+    prob, exp = gc.load(name)
+    s = solve_pdlp(prob, _params(name))
+    assert s.status == Status(int(exp.status)) == Status.OPTIMAL
+    ref = float(exp.objective)
+    assert abs(s.objective - ref) / max(1.0, abs(ref)) < 1e-6
+    if np.isfinite(exp.known):
+        known = float(exp.known)
+        assert abs(s.objective - known) / max(1.0, abs(known)) < 1e-6
+    v = vo.verify(prob, s.x, s.objective, feas_tol=1e-6)
+    assert v.ok, v.report()
+    it_ref = int(exp.iterations)
+    assert abs(s.iterations - it_ref) <= max(256, 0.25 * it_ref), (s.iterations, it_ref)
+    assert s.method == "pdlp[gpu]"
+    assert s.info.device == "gpu"
+    # the duals: strong duality against the reference's (same optimum)
+    np.testing.assert_allclose(s.y, exp.y, rtol=1e-3, atol=1e-3 * max(1.0, np.abs(exp.y).max()))
+
+
+def test_trajectory_follows_reference(require_gpu):
+    """max_iter=100: the iterate after 100 iterations equals the reference's."""
+    prob, exp = gc.load("small_known_iterlimit")
+    s = solve_pdlp(prob, _params("small_known_iterlimit"))
+    assert s.status == Status.ITERATION_LIMIT
+    assert s.iterations == 100
+    assert s.info.restarts == int(exp.restarts)
+    assert s.info.rejected_steps == int(exp.rejected)
+    np.testing.assert_allclose(s.x, exp.x, rtol=1e-8, atol=1e-9)
+    np.testing.assert_allclose(s.y, exp.y, rtol=1e-8, atol=1e-9)
+    assert s.info.step_size == pytest.approx(float(exp.step_size), rel=1e-9)
+    assert s.info.primal_weight == pytest.approx(float(exp.primal_weight), rel=1e-9)
+    hist = np.array(s.log).reshape(-1, 5)
+    np.testing.assert_allclose(hist, exp.history, rtol=1e-6, atol=1e-9)
+
+
+@pytest.mark.parametrize("name", ["badly_scaled_s0", "randlp_2000", "blend_mini"])
+def test_iteration_limited_cases(require_gpu, name):
+    prob, exp = gc.load(name)
+    s = solve_pdlp(prob, _params(name))
+    assert s.status == Status(int(exp.status))
+    assert s.iterations == int(exp.iterations)
+    ref = float(exp.objective)
+    assert abs(s.objective - ref) / max(1.0, abs(ref)) < 1e-3
+
+
+def test_known_answers(require_gpu):
+    prob, _ = gc.load("toy")
+    s = solve_pdlp(prob, PDLPParams(device="gpu"))
+    assert s.status == Status.OPTIMAL
+    assert abs(s.objective - 11.0) < 1e-6
+    assert np.allclose(s.x, [3.0, 1.0], atol=1e-5)
+    prob, _ = gc.load("testprob")
+    s = solve_pdlp(prob, PDLPParams(device="gpu"))
+    assert s.status == Status.OPTIMAL
+    assert abs(s.objective - 16.0) < 1e-7
+    assert np.allclose(s.x, [0.0, -1.0, 6.0], atol=1e-6)
+
+
+def test_maximise_and_minimise_agree(require_gpu):
+    p, _ = gc.load("toy")
+    q, _ = gc.load("toy_min")
+    a = solve_pdlp(p, PDLPParams(device="gpu"))
+    b = solve_pdlp(q, PDLPParams(device="gpu"))
+    assert abs(a.objective + b.objective) < 1e-5
+
+
+def test_strong_duality_after_unscaling(require_gpu):
+    """tests/test_solvers.py:69-99: the reported gap closes and complementary
+    slackness holds against the unscaled duals."""
+    prob, exp = gc.load("dual_regression")
+    s = solve_pdlp(prob, _params("dual_regression"))
+    assert s.status == Status.OPTIMAL
+    assert float(exp.scale_obj) != 1.0
+    assert s.info.gap <= 1e-4 * max(1.0, abs(s.objective))
+    act = prob.A.matvec(s.x)
+    slack = np.where(prob.row_ub < 1e30, prob.row_ub - act, 0.0)
+    assert float(np.max(np.abs(s.y) * np.abs(slack))) <= 1e-4 * max(1.0, abs(s.objective))
+
+
+def test_malformed_input_is_rejected(require_gpu):
+    from sovereign_moe_b200 import _lib
+    prob, _ = gc.load("small_known_s0")
+    bad = prob.copy()
+    bad.A.ri[5] = bad.A.n + 7                      # column index out of range
+    with pytest.raises(_lib.PDLPError) as e:
+        solve_pdlp(bad, PDLPParams(device="gpu"))
+    assert e.value.code == _lib.PDLP_ERR_ARG
+    bad = prob.copy()
+    bad.c[3] = np.nan
+    with pytest.raises(_lib.PDLPError) as e:
+        solve_pdlp(bad, PDLPParams(device="gpu"))
+    assert e.value.code == _lib.PDLP_ERR_NUMERICAL
+    bad = prob.copy()
+    bad.A.rp[3] = bad.A.rp[4] + 1                  # pointers not monotone
+    with pytest.raises(_lib.PDLPError) as e:
+        solve_pdlp(bad, PDLPParams(device="gpu"))
+    assert e.value.code == _lib.PDLP_ERR_ARG
+
+
+def test_time_limit_status(require_gpu):
+    prob, _ = gc.load("blend_mini")
+    s = solve_pdlp(prob, PDLPParams(device="gpu", eps_abs=1e-12, eps_rel=1e-12,
+                                    time_limit=0.2))
+    assert s.status == Status.TIME_LIMIT
+    assert np.isfinite(s.objective)
+    assert s.time < 5.0
+
+
+def test_batch_results_equal_alone(require_gpu):
+    """A slot's result does not depend on the other LPs in the launch."""
+    from sovereign_moe_b200.batch import BatchEngine
+    names = ["small_known_s0", "small_known_s1", "agree", "toy", "testprob"]
+    probs = [gc.load(n)[0] for n in names]
+    params = PDLPParams(device="gpu", eps_abs=1e-6, eps_rel=1e-6)
+    with BatchEngine(max_slots=8) as eng:
+        together = eng.solve_all(probs, params)
+    for p, t in zip(probs, together):
+        with BatchEngine(max_slots=1) as eng:
+            alone = eng.solve_all([p], params)[0]
+        assert t.status == alone.status
+        assert t.iterations == alone.iterations
+        assert np.array_equal(t.x, alone.x)
+        assert np.array_equal(t.y, alone.y)
+
+
+def test_persistent_and_per_pass_launch_agree(require_gpu):
+    from sovereign_moe_b200.batch import BatchEngine
+    prob, _ = gc.load("small_known_s1")
+    params = PDLPParams(device="gpu", eps_abs=1e-6, eps_rel=1e-6)
+    with BatchEngine(max_slots=1, persistent=True) as e1:
+        a = e1.solve_all([prob], params)[0]
+    with BatchEngine(max_slots=1, persistent=False) as e2:
+        b = e2.solve_all([prob], params)[0]
+    assert a.iterations == b.iterations
+    assert np.array_equal(a.x, b.x)

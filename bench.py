@@ -1,0 +1,439 @@
+"""Benchmark: LP solves/s at rel KKT 1e-6 on the batched B200 PDLP engine.
+
+Workload ("uneven_batch_256"): 256 synthetic LPs of uneven size, rows
+log-uniform in 50-5000, columns 2-8x rows, 4-12 nonzeros per column, N(0,1)
+values, each built around a known optimum (sovereign_moe_b200.workloads).
+One step solves the whole batch to the reference's termination test at
+eps_abs = eps_rel = 1e-6 (feas_cap 1e-6, unscaled problem) in one persistent
+launch sequence.  The metric is quoted on this batched configuration because
+it is a throughput of solves; the single large LP of the blending-plan
+configuration does not reach that tolerance within the reference's default
+iteration budget, so it serves the per-kernel roofline instead.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value   : solves/s with the LPs already resident in HBM (admission from device
+          memory, preconditioning, solve, unscaled solution written to device
+          memory), whole job over all ranks.
+e2e     : the same through the C ABI from pinned host buffers: H2D of every
+          LP's arrays, solve, D2H of x, y and reduced costs, inside the timing.
+roofline: the persistent engine kernel; algorithmic bytes of the PDHG
+          iterations it ran (24 nnz + 4(m+1) + 4(n+1) + 8(10m + 11n) per
+          iteration of an LP, float64) over its CUDA-event time.
+--impl reference: the CPU restatement of the reference path (oracle/, same
+          iterates as sovopt's solve_pdlp bit for bit) on a bounded sample of
+          the same LPs, all host threads, rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "uneven_batch_256"
+METRIC = "LP solves/s at rel KKT 1e-6"
+N_LP = 256
+EPS = 1e-6
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_batch(seed):
+    from sovereign_moe_b200.workloads import uneven_batch
+    return uneven_batch(seed=seed, count=N_LP)
+
+
+def params():
+    from sovereign_moe_b200.pdlp import PDLPParams
+    return PDLPParams(device="gpu", eps_abs=EPS, eps_rel=EPS)
+
+
+# --------------------------------------------------------------------------- #
+# clocks                                                                       #
+# --------------------------------------------------------------------------- #
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during timing."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    smax.append(float(f[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        os.unlink(self.path)
+        busy = [s for s in sm if smax and s > 0.3 * max(smax)] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# --------------------------------------------------------------------------- #
+# reference arm / CPU baseline                                                 #
+# --------------------------------------------------------------------------- #
+
+def cpu_sample(lps, budget_s):
+    """Solve LPs in order with the CPU oracle until ``budget_s`` is spent."""
+    from oracle import pdlp_oracle as po
+    t0 = time.perf_counter()
+    solved = 0
+    for k in lps:
+        s = po.solve_pdlp(k.problem, dict(eps_abs=EPS, eps_rel=EPS))
+        if s.status != po.OPTIMAL:
+            raise RuntimeError(f"oracle did not converge on {k.problem.name}")
+        solved += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return solved, dt, po.num_threads()
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    lps = make_batch(seed=1000)
+    budget = args.cpu_budget
+    for _ in range(args.warmup and 1):
+        cpu_sample(lps[:1], 0.0)                      # C kernels loaded, caches warm
+    rates, sample_info = [], None
+    for _ in range(args.steps):
+        solved, dt, cores = cpu_sample(lps, budget)
+        rates.append(solved / dt)
+        sample_info = (solved, dt, cores)
+    value = statistics.median(rates)
+    solved, dt, cores = sample_info
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * N_LP / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "lps_per_step": N_LP, "tolerance": "rel KKT 1e-6",
+                   "sample": f"first {solved} of {N_LP} LPs per step, {dt:.1f} s"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
+                         "sample": f"{solved} LPs of the {N_LP}-LP batch in {dt:.1f} s"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------- #
+# GPU arm                                                                      #
+# --------------------------------------------------------------------------- #
+
+def device_problem(prob, torch):
+    """Device-resident copies of one LP's arrays and a desc over them."""
+    from sovereign_moe_b200 import _lib
+    from sovereign_moe_b200.problem import ObjSense
+    A = prob.A
+    t = {
+        "rp": torch.as_tensor(A.rp, device="cuda"), "ri": torch.as_tensor(A.ri, device="cuda"),
+        "rx": torch.as_tensor(A.rx, device="cuda"), "cp": torch.as_tensor(A.cp, device="cuda"),
+        "ci": torch.as_tensor(A.ci, device="cuda"), "cx": torch.as_tensor(A.cx, device="cuda"),
+        "c": torch.as_tensor(prob.c, device="cuda"),
+        "row_lb": torch.as_tensor(prob.row_lb, device="cuda"),
+        "row_ub": torch.as_tensor(prob.row_ub, device="cuda"),
+        "col_lb": torch.as_tensor(prob.col_lb, device="cuda"),
+        "col_ub": torch.as_tensor(prob.col_ub, device="cuda"),
+        "v0": torch.as_tensor(np.random.default_rng(0).standard_normal(A.n), device="cuda"),
+    }
+    return t, _make_desc(prob, t, _lib.PDLP_MEM_DEVICE)
+
+
+def host_problem(prob, torch):
+    """Pinned host copies of one LP's arrays and a desc over them."""
+    from sovereign_moe_b200 import _lib
+    A = prob.A
+    arrays = {"rp": A.rp, "ri": A.ri, "rx": A.rx, "cp": A.cp, "ci": A.ci, "cx": A.cx,
+              "c": prob.c, "row_lb": prob.row_lb, "row_ub": prob.row_ub,
+              "col_lb": prob.col_lb, "col_ub": prob.col_ub,
+              "v0": np.random.default_rng(0).standard_normal(A.n)}
+    t = {k: torch.as_tensor(np.ascontiguousarray(v)).pin_memory() for k, v in arrays.items()}
+    return t, _make_desc(prob, t, _lib.PDLP_MEM_HOST)
+
+
+def _make_desc(prob, t, memory):
+    from sovereign_moe_b200 import _lib
+    from sovereign_moe_b200.problem import ObjSense
+    d = _lib.ProblemDesc()
+    d.m, d.n, d.nnz = int(prob.A.m), int(prob.A.n), int(prob.A.nnz)
+    for k in ("rp", "ri", "rx", "cp", "ci", "cx", "c", "row_lb", "row_ub", "col_lb", "col_ub"):
+        setattr(d, k, t[k].data_ptr())
+    d.kind = None
+    d.obj_offset = float(prob.obj_offset)
+    d.sense = -1 if int(prob.sense) == int(ObjSense.MAXIMISE) else 1
+    d.memory = memory
+    return d
+
+
+def h2d_bytes(prob):
+    m, n, nnz = prob.A.m, prob.A.n, prob.A.nnz
+    return 8 * (m + 1) + 8 * (n + 1) + 2 * 12 * nnz + 8 * (4 * n + 2 * m)
+
+
+class GpuArm:
+    def __init__(self, lps, torch, stream_ptr=None):
+        import ctypes
+        from sovereign_moe_b200 import _lib
+        from sovereign_moe_b200.batch import BatchEngine
+        from sovereign_moe_b200.pdlp import params_struct
+        self.ctypes = ctypes
+        self._lib = _lib
+        self.lps = lps
+        self.torch = torch
+        self.eng = BatchEngine(max_slots=len(lps))
+        self.lib = self.eng.lib
+        self.p = params()
+        self.dev = [device_problem(k.problem, torch) for k in lps]
+        self.host = [host_problem(k.problem, torch) for k in lps]
+        self.params = []
+        for k, (t, _) in zip(lps, self.dev):
+            ps, _keep = params_struct(self.p, int(k.problem.A.n), power_start=None,
+                                      history_capacity=0)
+            ps.power_start = t["v0"].data_ptr()
+            self.params.append(ps)
+        self.hparams = []
+        for k, (t, _) in zip(lps, self.host):
+            ps, _keep = params_struct(self.p, int(k.problem.A.n), power_start=None,
+                                      history_capacity=0)
+            ps.power_start = t["v0"].data_ptr()
+            self.hparams.append(ps)
+        self.out_dev = [(torch.empty(k.problem.A.n, dtype=torch.float64, device="cuda"),
+                         torch.empty(k.problem.A.m, dtype=torch.float64, device="cuda"),
+                         torch.empty(k.problem.A.n, dtype=torch.float64, device="cuda"))
+                        for k in lps]
+        self.out_host = [(torch.empty(k.problem.A.n, dtype=torch.float64).pin_memory(),
+                          torch.empty(k.problem.A.m, dtype=torch.float64).pin_memory(),
+                          torch.empty(k.problem.A.n, dtype=torch.float64).pin_memory())
+                         for k in lps]
+        self.engine_ms = 0.0
+        self.engine_bytes = 0.0
+        self.engine_launches = 0
+
+    def step(self, host=False):
+        ct, L, c = self.ctypes, self._lib, self.lib
+        descs = self.host if host else self.dev
+        prms = self.hparams if host else self.params
+        outs = self.out_host if host else self.out_dev
+        mem = L.PDLP_MEM_HOST if host else L.PDLP_MEM_DEVICE
+        slots = []
+        for (t, d), p in zip(descs, prms):
+            s = ct.c_int32(-1)
+            L.check(c.pdlp_batch_admit(self.eng.h, ct.byref(d), ct.byref(p), ct.byref(s)))
+            slots.append(s.value)
+        active = ct.c_int32(1)
+        while active.value > 0:
+            L.check(c.pdlp_batch_step(self.eng.h, 1 << 16, ct.byref(active)))
+            ms, by, _ = self.eng.last_timing()
+            self.engine_ms += ms
+            self.engine_bytes += by
+            self.engine_launches += 1
+        statuses = []
+        for s, (x, y, dd) in zip(slots, outs):
+            r = L.Result()
+            L.check(c.pdlp_batch_poll(self.eng.h, s, ct.byref(r)))
+            statuses.append(r.status)
+            L.check(c.pdlp_batch_fetch(self.eng.h, s, x.data_ptr(), y.data_ptr(), dd.data_ptr(),
+                                       None, mem))
+            L.check(c.pdlp_batch_retire(self.eng.h, s))
+        return statuses
+
+
+def verify_batch(arm, lps):
+    """Every result of the last device-resident step against its known optimum
+    and the independent verifier."""
+    from oracle import verify_oracle as vo
+    worst = 0.0
+    for k, (x, y, d) in zip(lps, arm.out_dev):
+        xh = x.cpu().numpy()
+        obj = float(k.problem.c @ xh) + k.problem.obj_offset
+        rel = abs(obj - k.f_star) / max(1.0, abs(k.f_star))
+        worst = max(worst, rel)
+        v = vo.verify(k.problem, xh, obj, feas_tol=1e-6)
+        if not v.ok or rel > 1e-6:
+            raise RuntimeError(f"{k.problem.name}: rel err {rel:.2e}\n{v.report()}")
+    return worst
+
+
+def run_gpu(args, rank, world):
+    import torch
+    import torch.distributed as dist
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from sovereign_moe_b200 import _lib
+    lib = _lib.load()
+
+    lps = make_batch(seed=1000 + rank)
+    arm = GpuArm(lps, torch)
+    for _ in range(args.warmup):
+        st = arm.step(host=False)
+    if any(s != 0 for s in st):
+        raise RuntimeError(f"warm-up statuses {set(st)}")
+    worst = verify_batch(arm, lps)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # device-resident timing
+    clocks = ClockSampler(local)
+    clocks.start()
+    arm.engine_ms = arm.engine_bytes = 0.0
+    arm.engine_launches = 0
+    n0 = lib.pdlp_launch_count()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        st = arm.step(host=False)
+    ev1.record()
+    barrier()
+    launches = lib.pdlp_launch_count() - n0
+    clk = clocks.stop()
+    dev_ms = ev0.elapsed_time(ev1)
+    step_ms = max_over_ranks(dev_ms / args.steps)
+    value = N_LP * world / (step_ms / 1000.0)
+    eng_ms, eng_bytes, eng_launches = arm.engine_ms, arm.engine_bytes, arm.engine_launches
+
+    # end to end through the C ABI from pinned host buffers
+    barrier()
+    ev0.record()
+    for _ in range(args.steps):
+        arm.step(host=True)
+    ev1.record()
+    barrier()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+    e2e = N_LP * world / (e2e_ms / 1000.0)
+    h2d = sum(h2d_bytes(k.problem) for k in lps)
+    d2h = sum(8 * (2 * k.problem.A.n + k.problem.A.m) for k in lps)
+
+    peak, peak_kind = load_peaks()
+    achieved = eng_bytes / (eng_ms / 1000.0) / 1e9 if eng_ms > 0 else 0.0
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        solved, dt, cores = cpu_sample(lps, args.cpu_budget)
+        cpu = {"value": solved / dt, "unit": "solves/s", "cores": cores, "kind": "port",
+               "sample": f"{solved} of the {N_LP} LPs solved in order by the CPU "
+                         f"restatement in {dt:.1f} s"}
+
+    if rank == 0:
+        total_nnz = sum(k.problem.A.nnz for k in lps)
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "lps_per_step": N_LP,
+                       "rows": "log-uniform 50-5000", "cols": "U{2..8} x rows",
+                       "nnz_per_col": "4-12", "total_nnz": int(total_nnz),
+                       "tolerance": "rel KKT 1e-6 (eps_abs=eps_rel=1e-6, feas_cap=1e-6)",
+                       "l2": "inputs larger than L2 (>126 MB of matrix data per step)",
+                       "parallelism": f"replicas x{world}", "worst_rel_obj_err": worst},
+            "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "engine_persistent", "peak_source": peak_kind,
+                         "launches": eng_launches, "kernel_ms_per_step": eng_ms / args.steps},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": int(launches),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    arm.eng.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=15.0,
+                    help="seconds of CPU work per timed CPU sample")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        ap.error("--warmup must be >= 3")
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.impl == "ours" else 1)))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_gpu(args, rank, world)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

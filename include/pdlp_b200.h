@@ -113,6 +113,10 @@ typedef struct pdlp_result {
 /* ---- library ---------------------------------------------------------- */
 int pdlp_abi_version(void);
 const char* pdlp_last_error(void);
+/* Number of kernels this library has launched in the process so far (all
+ * entry points); lets a caller count the GPU launches inside a timed region.
+ * No counterpart in the reference (its kernels are CuPy RawModule calls). */
+int64_t pdlp_launch_count(void);
 
 /* ---- whole solve: solve_pdlp (pdlp.py:238-494) ------------------------- *
  * Solves one LP: scaling, PDHG, restarts and termination all run on the
@@ -161,6 +165,11 @@ int pdlp_batch_poll(pdlp_batch* b, int32_t slot, pdlp_result* result);
 /* Copies a finished slot's solution out (pointers in `memory`; NULL skips). */
 int pdlp_batch_fetch(pdlp_batch* b, int32_t slot, double* x, double* y,
                      double* reduced_costs, double* history, int32_t memory);
+/* Status of every slot as of the last pdlp_batch_step (no device access):
+ * status_out[s] for s < n is PDLP_STATUS_RUNNING, a final status, or
+ * PDLP_SLOT_FREE for an unused slot. */
+#define PDLP_SLOT_FREE -2
+int pdlp_batch_statuses(pdlp_batch* b, int32_t* status_out, int32_t n);
 /* Releases a slot's device memory. */
 int pdlp_batch_retire(pdlp_batch* b, int32_t slot);
 /* Requests the slot to stop at its next check (status INTERRUPTED). */

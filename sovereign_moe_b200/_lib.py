@@ -25,6 +25,7 @@ PDLP_MEM_DEVICE = 0
 PDLP_MEM_HOST = 1
 
 PDLP_STATUS_RUNNING = -1
+PDLP_SLOT_FREE = -2
 
 SCALING = {"pdlp": 0, "none": 1, "ruiz": 2, "pock_chambolle": 3}
 
@@ -75,6 +76,7 @@ _i32, _i64, _d = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
 SIGNATURES = {
     "pdlp_abi_version": ([], ctypes.c_int),
     "pdlp_last_error": ([], ctypes.c_char_p),
+    "pdlp_launch_count": ([], ctypes.c_int64),
     "pdlp_params_default": ([ctypes.POINTER(Params)], None),
     "pdlp_solve": ([ctypes.POINTER(ProblemDesc), ctypes.POINTER(Params), _c_p,
                     ctypes.POINTER(Result), _c_p, _c_p, _c_p, _c_p, _i32], ctypes.c_int),
@@ -87,6 +89,7 @@ SIGNATURES = {
     "pdlp_batch_poll": ([_c_p, _i32, ctypes.POINTER(Result)], ctypes.c_int),
     "pdlp_batch_fetch": ([_c_p, _i32, _c_p, _c_p, _c_p, _c_p, _i32], ctypes.c_int),
     "pdlp_batch_retire": ([_c_p, _i32], ctypes.c_int),
+    "pdlp_batch_statuses": ([_c_p, _c_p, _i32], ctypes.c_int),
     "pdlp_batch_cancel": ([_c_p, _i32], ctypes.c_int),
     "pdlp_slot_bytes": ([_i32, _i32, _i64], ctypes.c_int64),
     "pdlp_batch_last_timing": ([_c_p, ctypes.POINTER(_d), ctypes.POINTER(_d),

@@ -104,6 +104,13 @@ class BatchEngine:
     def done(self, slot):
         return self.poll(slot).status != _lib.PDLP_STATUS_RUNNING
 
+    def statuses(self):
+        """Status of every slot as of the last ``step`` (no device access):
+        ``PDLP_STATUS_RUNNING``, a final status, or ``PDLP_SLOT_FREE``."""
+        out = np.empty(self.max_slots, dtype=np.int32)
+        _lib.check(self.lib.pdlp_batch_statuses(self.h, out.ctypes.data, self.max_slots))
+        return out
+
     def fetch(self, slot):
         """The finished slot's result as a reference ``Solution``."""
         prob, params, hcap, t0 = self._meta[slot]

@@ -14,6 +14,9 @@ namespace pdlp {
 void set_error(const std::string& msg);
 const std::string& get_error();
 
+// Kernel launches made by the library (pdlp_launch_count()).
+void count_launches(long long n);
+
 inline int fail(int code, const std::string& msg) {
   set_error(msg);
   return code;

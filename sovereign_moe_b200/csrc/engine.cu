@@ -1,6 +1,8 @@
 // PDLP engine: kernels (persistent cooperative and per-pass) and the batch
 // runtime behind the C ABI (admission, tile planning, launch, polling).
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -50,8 +52,12 @@ __device__ bool grid_barrier(Control* ctl, unsigned nblocks, long long timeout_n
   return sm.flag != 0;
 }
 
+extern __shared__ __align__(16) unsigned char g_smem[];
+
 __global__ void __launch_bounds__(kBlock) engine_persistent(EngineArgs A) {
-  __shared__ Smem sm;
+  Smem& sm = *reinterpret_cast<Smem*>(g_smem);
+  if (threadIdx.x == 0) sm.inst_id = -1;
+  __syncthreads();
   const unsigned nb = gridDim.x;
   const int b = blockIdx.x;
   const int r0 = A.rblock[b], r1 = A.rblock[b + 1];
@@ -70,7 +76,9 @@ __global__ void __launch_bounds__(kBlock) engine_persistent(EngineArgs A) {
 
 // One pass over all tiles of one side; kernel boundaries are the barriers.
 __global__ void __launch_bounds__(kBlock) engine_pass(EngineArgs A, int side) {
-  __shared__ Smem sm;
+  Smem& sm = *reinterpret_cast<Smem*>(g_smem);
+  if (threadIdx.x == 0) sm.inst_id = -1;
+  __syncthreads();
   if (side == 0) {
     for (int t = blockIdx.x; t < A.n_rtiles; t += gridDim.x) process_rtile(A, t, sm);
   } else {
@@ -124,8 +132,8 @@ constexpr size_t kAlign = 256;
 size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
 int default_tile_rows() { return 512; }
-int default_tile_nnz() { return 8192; }
-int heavy_threshold() { return 4096; }
+int default_tile_nnz() { return kTileNnz; }
+int heavy_threshold() { return kTileNnz; }   // longer rows: a block-wide tile alone
 
 int lanes_for(long long nnz, long long rows) {
   if (rows <= 0) return 1;
@@ -217,6 +225,9 @@ namespace pdlp {
 
 void set_error(const std::string& msg) { g_err = msg; }
 const std::string& get_error() { return g_err; }
+
+static std::atomic<long long> g_launches{0};
+void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 }  // namespace pdlp
 
@@ -357,6 +368,8 @@ extern "C" {
 
 int pdlp_abi_version(void) { return PDLP_ABI_VERSION; }
 
+int64_t pdlp_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
 const char* pdlp_last_error(void) { return g_err.c_str(); }
 
 void pdlp_params_default(pdlp_params* p) {
@@ -405,6 +418,7 @@ int pdlp_batch_create(const pdlp_batch_config* cfg, void* stream, pdlp_batch** o
   if (c.tile_rows <= 0) c.tile_rows = default_tile_rows();
   if (c.tile_rows > kMaxTileRows) return fail(PDLP_ERR_ARG, "tile_rows exceeds 1024");
   if (c.tile_nnz <= 0) c.tile_nnz = default_tile_nnz();
+  if (c.tile_nnz > kTileNnz) return fail(PDLP_ERR_ARG, "tile_nnz exceeds 4096");
   if (c.lanes_override && (c.lanes_override & (c.lanes_override - 1)))
     return fail(PDLP_ERR_ARG, "lanes_override must be a power of two");
   pdlp_batch* b = new pdlp_batch();
@@ -423,8 +437,14 @@ int pdlp_batch_create(const pdlp_batch_config* cfg, void* stream, pdlp_batch** o
     return bail(e, "cudaDeviceGetAttribute");
   int coop = 0;
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  if ((e = cudaFuncSetAttribute(engine_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(Smem))) != cudaSuccess)
+    return bail(e, "cudaFuncSetAttribute");
+  if ((e = cudaFuncSetAttribute(engine_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(Smem))) != cudaSuccess)
+    return bail(e, "cudaFuncSetAttribute");
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->coop_blocks_per_sm, engine_persistent,
-                                                          kBlock, 0)) != cudaSuccess)
+                                                          kBlock, sizeof(Smem))) != cudaSuccess)
     return bail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
   if (!coop || b->coop_blocks_per_sm < 1) b->cfg.persistent = 0;
   if ((e = cudaMalloc(&b->d_inst, sizeof(Inst) * c.max_slots)) != cudaSuccess) return bail(e, "cudaMalloc");
@@ -565,6 +585,7 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
     check_finite<<<grid_for(m), 256, 0, st>>>((const double*)at(L.rl0), m, 1, err_flag);
     check_finite<<<grid_for(m), 256, 0, st>>>((const double*)at(L.ru0), m, 1, err_flag);
   }
+  count_launches(2 + (nnz > 0 ? 4 : 0) + (n > 0 ? 3 : 0) + (m > 0 ? 2 : 0));
   int herr = 0;
   PDLP_CUDA(cudaMemcpyAsync(&herr, err_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
   e = cudaStreamSynchronize(st);
@@ -638,67 +659,79 @@ int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out) {
   b->last_ms = 0.0; b->last_bytes = 0.0; b->last_iters = 0;
   if (b->n_running == 0) { if (active_out) *active_out = 0; return PDLP_OK; }
   int rc;
-  if (b->dirty && (rc = rebuild(b))) return rc;
   cudaStream_t st = b->stream;
   EngineArgs A{};
   A.inst = b->d_inst; A.st = b->d_state;
-  A.rtiles = b->d_rtiles; A.n_rtiles = b->n_rtiles;
-  A.ctiles = b->d_ctiles; A.n_ctiles = b->n_ctiles;
-  A.rblock = b->d_rblock; A.cblock = b->d_cblock;
-  A.partials = b->d_partials; A.counters = b->d_counters; A.ctl = b->d_ctl;
-  A.max_steps = max_steps;
+  A.counters = b->d_counters; A.ctl = b->d_ctl;
   A.barrier_timeout_ns = 4000000000LL;
   A.n_inst = (int)b->slots.size();
-  b->h_ctl->bar_count = 0; b->h_ctl->bar_gen = 0; b->h_ctl->active = b->n_running;
-  b->h_ctl->error = 0; b->h_ctl->error_where = 0;
-  PDLP_CUDA(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(Control), cudaMemcpyHostToDevice, st));
-  PDLP_CUDA(cudaEventRecord(b->ev0, st));
-  if (b->cfg.persistent) {
-    void* args[] = {&A};
-    PDLP_CUDA(cudaLaunchCooperativeKernel((void*)engine_persistent, dim3(b->grid), dim3(kBlock),
-                                          args, 0, st));
-  } else {
-    // one launch per pass, in chunks; the engine is idle once every LP is done
-    const int g_r = std::max(1, std::min(b->n_rtiles, b->sms * 8));
-    const int g_c = std::max(1, std::min(b->n_ctiles, b->sms * 8));
-    const int64_t chunk = 64;
-    for (int64_t done = 0; done < max_steps; done += chunk) {
-      const int64_t k = std::min(chunk, max_steps - done);
-      for (int64_t s = 0; s < k; ++s) {
-        engine_pass<<<g_r, kBlock, 0, st>>>(A, 0);
-        engine_pass<<<g_c, kBlock, 0, st>>>(A, 1);
+  // Chunks of at most kChunk steps: between chunks the host drops finished
+  // LPs from the tile lists and re-balances the blocks over what is left.
+  const int64_t kChunk = 256;
+  int64_t left = max_steps;
+  double total_ms = 0.0;
+  while (left > 0 && b->n_running > 0) {
+    if (b->dirty && (rc = rebuild(b))) return rc;
+    A.rtiles = b->d_rtiles; A.n_rtiles = b->n_rtiles;
+    A.ctiles = b->d_ctiles; A.n_ctiles = b->n_ctiles;
+    A.rblock = b->d_rblock; A.cblock = b->d_cblock;
+    A.partials = b->d_partials;
+    const int64_t chunk = std::min(left, kChunk);
+    left -= chunk;
+    A.max_steps = chunk;
+    b->h_ctl->bar_count = 0; b->h_ctl->bar_gen = 0; b->h_ctl->active = b->n_running;
+    b->h_ctl->error = 0; b->h_ctl->error_where = 0;
+    PDLP_CUDA(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(Control), cudaMemcpyHostToDevice, st));
+    PDLP_CUDA(cudaEventRecord(b->ev0, st));
+    if (b->cfg.persistent) {
+      void* args[] = {&A};
+      PDLP_CUDA(cudaLaunchCooperativeKernel((void*)engine_persistent, dim3(b->grid), dim3(kBlock),
+                                            args, sizeof(Smem), st));
+      count_launches(1);
+    } else {
+      const int g_r = std::max(1, std::min(b->n_rtiles, b->sms * b->coop_blocks_per_sm));
+      const int g_c = std::max(1, std::min(b->n_ctiles, b->sms * b->coop_blocks_per_sm));
+      for (int64_t s = 0; s < chunk; ++s) {
+        engine_pass<<<g_r, kBlock, sizeof(Smem), st>>>(A, 0);
+        engine_pass<<<g_c, kBlock, sizeof(Smem), st>>>(A, 1);
       }
+      count_launches(2 * chunk);
       PDLP_CUDA(cudaGetLastError());
-      PDLP_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, st));
-      PDLP_CUDA(cudaStreamSynchronize(st));
-      if (b->h_ctl->active <= 0) break;
     }
+    PDLP_CUDA(cudaEventRecord(b->ev1, st));
+    PDLP_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, st));
+    PDLP_CUDA(cudaMemcpyAsync(b->h_state, b->d_state, sizeof(State) * b->slots.size(),
+                              cudaMemcpyDeviceToHost, st));
+    PDLP_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    total_ms += ms;
+    if (b->h_ctl->error) {
+      b->broken = true;
+      return fail(b->h_ctl->error, "engine: a bounded grid barrier timed out; the batch was stopped");
+    }
+    int running = 0;
+    for (size_t s = 0; s < b->slots.size(); ++s) {
+      Slot& sl = b->slots[s];
+      if (!sl.used || !sl.running) continue;
+      const State& hs = b->h_state[s];
+      long long d = hs.iters_done - b->iters_before[s];
+      b->iters_before[s] = hs.iters_done;
+      b->last_iters += d;
+      b->last_bytes += d * sl.bytes_per_iter;
+      if (hs.status != PDLP_STATUS_RUNNING) { sl.running = false; b->dirty = true; }
+      else {
+        ++running;
+        if (hs.rmode == R_NONE && hs.cmode == C_NONE) {
+          b->broken = true;
+          return fail(PDLP_ERR_STATE, "engine: a running LP has no pass scheduled (internal error)");
+        }
+      }
+    }
+    b->n_running = running;
   }
-  PDLP_CUDA(cudaEventRecord(b->ev1, st));
-  PDLP_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, st));
-  PDLP_CUDA(cudaMemcpyAsync(b->h_state, b->d_state, sizeof(State) * b->slots.size(), cudaMemcpyDeviceToHost, st));
-  PDLP_CUDA(cudaStreamSynchronize(st));
-  float ms = 0.f;
-  cudaEventElapsedTime(&ms, b->ev0, b->ev1);
-  b->last_ms = ms;
-  if (b->h_ctl->error) {
-    b->broken = true;
-    return fail(b->h_ctl->error, "engine: a bounded grid barrier timed out; the batch was stopped");
-  }
-  int running = 0;
-  for (size_t s = 0; s < b->slots.size(); ++s) {
-    Slot& sl = b->slots[s];
-    if (!sl.used || !sl.running) continue;
-    const State& hs = b->h_state[s];
-    long long d = hs.iters_done - b->iters_before[s];
-    b->iters_before[s] = hs.iters_done;
-    b->last_iters += d;
-    b->last_bytes += d * sl.bytes_per_iter;
-    if (hs.status != PDLP_STATUS_RUNNING) { sl.running = false; b->dirty = true; }
-    else ++running;
-  }
-  b->n_running = running;
-  if (active_out) *active_out = running;
+  b->last_ms = total_ms;
+  if (active_out) *active_out = b->n_running;
   return PDLP_OK;
 }
 
@@ -760,6 +793,16 @@ int pdlp_batch_fetch(pdlp_batch* b, int32_t slot, double* x, double* y, double* 
   return PDLP_OK;
 }
 
+int pdlp_batch_statuses(pdlp_batch* b, int32_t* out, int32_t n) {
+  if (!b || (!out && n > 0)) return fail(PDLP_ERR_ARG, "NULL argument");
+  for (int32_t s = 0; s < n; ++s) {
+    if (s >= (int)b->slots.size() || !b->slots[s].used) out[s] = PDLP_SLOT_FREE;
+    else if (b->slots[s].running) out[s] = PDLP_STATUS_RUNNING;
+    else out[s] = b->h_state[s].status;
+  }
+  return PDLP_OK;
+}
+
 int pdlp_batch_retire(pdlp_batch* b, int32_t slot) {
   if (!b) return fail(PDLP_ERR_ARG, "NULL batch");
   if (slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
@@ -796,8 +839,15 @@ int pdlp_solve(const pdlp_problem_desc* prob, const pdlp_params* params, void* s
   int slot = -1;
   if ((rc = pdlp_batch_admit(b, prob, params, &slot))) { pdlp_batch_destroy(b); return rc; }
   int active = 1;
+  const double guard_s = (params ? params->time_limit : 600.0) + 120.0;
+  const auto t0 = std::chrono::steady_clock::now();
   while (active > 0) {
-    if ((rc = pdlp_batch_step(b, 1 << 20, &active))) { pdlp_batch_destroy(b); return rc; }
+    if ((rc = pdlp_batch_step(b, 1 << 16, &active))) { pdlp_batch_destroy(b); return rc; }
+    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (active > 0 && el > guard_s) {
+      pdlp_batch_destroy(b);
+      return fail(PDLP_ERR_STATE, "engine: the solve outran its time limit by two minutes");
+    }
   }
   pdlp_result r;
   if ((rc = pdlp_batch_poll(b, slot, &r))) { pdlp_batch_destroy(b); return rc; }

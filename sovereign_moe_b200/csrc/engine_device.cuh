@@ -15,14 +15,20 @@ namespace pdlp {
 
 constexpr int kBlock = 256;            // threads per block (all engine kernels)
 constexpr int kMaxTileRows = 1024;     // rows per tile (shared-memory staging)
+constexpr int kTileNnz = 4096;         // entries per normal tile (products staged in smem)
 constexpr double kRuizTol = 1e-2;      // scaling.py:149
 constexpr unsigned kFull = 0xffffffffu;
 
+// Per-block shared memory (dynamic: larger than the 48 KB static limit).
 struct Smem {
-  double s0[kMaxTileRows];
-  double s1[kMaxTileRows];
+  double prod[kTileNnz];               // products of the tile's entries
+  double s0[kMaxTileRows];             // row sums, first right-hand side
+  double s1[kMaxTileRows];             // row sums, second right-hand side
+  int ptr[kMaxTileRows + 1];           // the tile's row pointers
   double red[32 * kNP];
   double res[kNP];
+  Inst inst;                           // cached descriptor of inst_id
+  int inst_id;
   int flag;
 };
 
@@ -118,10 +124,72 @@ __device__ __forceinline__ void heavy_spmv(const int* __restrict__ ptr, int r, F
   __syncthreads();
 }
 
+// Row sums of a normal tile, CSR-stream style: every entry's product is
+// computed first (all loads and gathers of the tile independent of each
+// other), staged in shared memory, then each row is summed from there by L
+// lanes (each lane its strided entries in storage order, then a xor
+// butterfly; L == 1 is the sequential storage-order sum).  The order depends
+// only on the row and on L, never on the tile or the batch.
+// term(p, rhs) returns value[p] * x_rhs[index[p]].
 template <int NR, class F>
-__device__ __forceinline__ void tile_spmv(const Tile& t, const int* ptr, int L, F f, Smem& sm) {
-  if (t.heavy) heavy_spmv<NR>(ptr, t.begin, f, sm.s0, sm.s1, sm);
-  else rows_spmv<NR>(ptr, t.begin, t.end, L, f, sm.s0, sm.s1);
+__device__ __forceinline__ void stream_spmv(const Tile& t, int L, F term, Smem& sm) {
+  const int tid = threadIdx.x, BT = blockDim.x;
+  const int rows = t.end - t.begin;
+  const int p0 = sm.ptr[0];
+  const int cnt = sm.ptr[rows] - p0;
+#pragma unroll 1
+  for (int rhs = 0; rhs < NR; ++rhs) {
+    for (int q0 = 0; q0 < cnt; q0 += 4 * BT) {
+      double v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int q = q0 + u * BT + tid;
+        v[u] = q < cnt ? term(p0 + q, rhs) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int q = q0 + u * BT + tid;
+        if (q < cnt) sm.prod[q] = v[u];
+      }
+    }
+    __syncthreads();
+    double* out = rhs == 0 ? sm.s0 : sm.s1;
+    const int lane = tid & (L - 1);
+    const int grp = tid / L, ngrp = BT / L;
+    for (int rb = 0; rb < rows; rb += ngrp) {
+      const int li = rb + grp;
+      double a = 0.0;
+      if (li < rows) {
+        const int e = sm.ptr[li + 1] - p0;
+        for (int q = sm.ptr[li] - p0 + lane; q < e; q += L) a += sm.prod[q];
+      }
+      for (int off = L >> 1; off > 0; off >>= 1) a += __shfl_xor_sync(kFull, a, off);
+      if (li < rows && lane == 0) out[li] = a;
+    }
+    __syncthreads();
+  }
+}
+
+// Loads the tile's row pointers into shared memory (normal tiles).
+__device__ __forceinline__ void load_tile_ptr(const Tile& t, const int* ptr, Smem& sm) {
+  if (t.heavy) return;
+  const int rows = t.end - t.begin;
+  for (int i = threadIdx.x; i <= rows; i += blockDim.x) sm.ptr[i] = ld_ro(ptr + t.begin + i);
+  __syncthreads();
+}
+
+template <int NR, class F>
+__device__ __forceinline__ void tile_spmv(const Tile& t, const int* ptr, int L, F term, Smem& sm) {
+  if (t.heavy) {
+    auto f = [&](int r, int p, double& a0, double& a1) {
+      a0 += term(p, 0);
+      if (NR == 2) a1 += term(p, 1);
+    };
+    heavy_spmv<NR>(ptr, t.begin, f, sm.s0, sm.s1, sm);
+  } else {
+    load_tile_ptr(t, ptr, sm);
+    stream_spmv<NR>(t, L, term, sm);
+  }
   __syncthreads();
 }
 

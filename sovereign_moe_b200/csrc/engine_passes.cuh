@@ -56,9 +56,9 @@ __device__ __forceinline__ double merit(double omega, double p, double d, double
 // block that completed the instance's last tile of this pass; that block then
 // sees every tile's partials.
 __device__ __forceinline__ bool finisher_enter(unsigned* cnt, int ntiles, Smem& sm) {
-  __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
+    __threadfence();            // this block's tile partials (written by thread 0)
     unsigned old = atomicAdd(cnt, 1u);
     sm.flag = (old == (unsigned)(ntiles - 1));
   }
@@ -132,12 +132,27 @@ __device__ void r_finish(const EngineArgs& A, const Inst& I, State* S, int rmode
   }
 }
 
+// Copy the tile's instance descriptor into shared memory (once per run of
+// tiles of the same instance).
+__device__ __forceinline__ const Inst& cache_inst(const EngineArgs& A, int inst, Smem& sm) {
+  const bool need = sm.inst_id != inst;
+  __syncthreads();
+  if (need) {
+    const int* src = reinterpret_cast<const int*>(A.inst + inst);
+    int* dst = reinterpret_cast<int*>(&sm.inst);
+    for (int i = threadIdx.x; i < (int)(sizeof(Inst) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    if (threadIdx.x == 0) sm.inst_id = inst;
+  }
+  return sm.inst;
+}
+
 __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
   const Tile t = A.rtiles[ti];
-  const Inst& I = A.inst[t.inst];
   State* S = A.st + t.inst;
   const int rmode = ld_mut(&S->rmode);
   if (rmode == R_NONE) return;
+  const Inst& I = cache_inst(A, t.inst, sm);
 
   const int L = I.lanes_r;
   const int* __restrict__ rp = I.rp;
@@ -247,18 +262,14 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
       const double scale = ld_mut(&S->power_scale);
       const double* v = I.xbar;                    // A^T A power vector
       const double* rx = I.rx;
-      if (round == 1) {
-        tile_spmv<2>(t, rp, L, [&](int r, int p, double& a0, double& a1) {
-          const int j = ld_ro(ri + p);
-          const double a = ld_mut(rx + p);
-          a0 += a * (scale != 0.0 ? ld_mut(v + j) / scale : 0.0);
-          a1 += a * ld_mut(I.x + j);
-        }, sm);
-      } else {
-        tile_spmv<1>(t, rp, L, [&](int r, int p, double& a0, double&) {
-          a0 += ld_mut(rx + p) * (ld_mut(v + ld_ro(ri + p)) / scale);
-        }, sm);
-      }
+      auto term = [&](int p, int rhs) {
+        const int j = ld_ro(ri + p);
+        const double a = ld_mut(rx + p);
+        if (rhs == 0) return a * (scale != 0.0 ? ld_mut(v + j) / scale : 0.0);
+        return a * ld_mut(I.x + j);
+      };
+      if (round == 1) tile_spmv<2>(t, rp, L, term, sm);
+      else tile_spmv<1>(t, rp, L, term, sm);
       ops.maxmask = 1u;
       for (int r = t.begin + threadIdx.x; r < rend; r += blockDim.x) {
         const int li = r - t.begin;
@@ -274,8 +285,9 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
     case R_ITER: {
       // backend.py:260-279: ax += adx; w = y + sigma (ax + adx); prox; dy
       const double* rx = I.rx;
-      tile_spmv<1>(t, rp, L, [&](int r, int p, double& a0, double&) {
-        a0 += ld_mut(rx + p) * ld_mut(I.dx + ld_ro(ri + p));
+      const double* dxv = I.dx;
+      tile_spmv<1>(t, rp, L, [&](int p, int) {
+        return ld_mut(rx + p) * ld_mut(dxv + ld_ro(ri + p));
       }, sm);
       for (int r = t.begin + threadIdx.x; r < rend; r += blockDim.x) {
         do_commit(r);
@@ -294,8 +306,9 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
     case R_TRIAL: {
       // pdlp.py:347-356: adx = A dx; ax_bar = ax + 2 adx; dual_step; dy; dots
       const double* rx = I.rx;
-      tile_spmv<1>(t, rp, L, [&](int r, int p, double& a0, double&) {
-        a0 += ld_mut(rx + p) * ld_mut(I.dx + ld_ro(ri + p));
+      const double* dxv = I.dx;
+      tile_spmv<1>(t, rp, L, [&](int p, int) {
+        return ld_mut(rx + p) * ld_mut(dxv + ld_ro(ri + p));
       }, sm);
       for (int r = t.begin + threadIdx.x; r < rend; r += blockDim.x) {
         do_commit(r);
@@ -333,11 +346,11 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
     }
     case R_CHECK_B: {
       const double* rx = I.rx;
-      tile_spmv<2>(t, rp, L, [&](int r, int p, double& a0, double& a1) {
+      const double* xb = I.xbar;
+      const double* xc = I.x;
+      tile_spmv<2>(t, rp, L, [&](int p, int rhs) {
         const int j = ld_ro(ri + p);
-        const double a = ld_mut(rx + p);
-        a0 += a * ld_mut(I.xbar + j);
-        a1 += a * ld_mut(I.x + j);
+        return ld_mut(rx + p) * ld_mut((rhs == 0 ? xb : xc) + j);
       }, sm);
       ops.maxmask = 7u;
       for (int r = t.begin + threadIdx.x; r < rend; r += blockDim.x) {
@@ -378,14 +391,23 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
     default: break;
   }
 
-  block_reduce(acc, ops, sm);
-  if (threadIdx.x == 0) {
+  // R_ITER carries no reduction, and needs its finisher only to retire a
+  // pending commit; the other modes reduce and/or advance the state machine.
+  const bool need_red = rmode == R_RUIZ || rmode == R_APPLY || rmode == R_POWER ||
+                        rmode == R_TRIAL || rmode == R_CHECK_A || rmode == R_CHECK_B;
+  const bool need_fin = !(rmode == R_ITER && !commit);
+  if (need_red) {
+    block_reduce(acc, ops, sm);
+    if (threadIdx.x == 0) {
 #pragma unroll
-    for (int s = 0; s < kNP; ++s) A.partials[(size_t)ti * kNP + s] = sm.res[s];
+      for (int s = 0; s < kNP; ++s) A.partials[(size_t)ti * kNP + s] = sm.res[s];
+    }
   }
+  if (!need_fin) return;
   const int ntiles = I.rt_end - I.rt_begin;
+  const int rt0 = I.rt_begin, rt1 = I.rt_end;
   if (finisher_enter(A.counters + 2 * t.inst, ntiles, sm)) {
-    reduce_tiles(A.partials, I.rt_begin, I.rt_end, ops, sm);
+    if (need_red) reduce_tiles(A.partials, rt0, rt1, ops, sm);
     if (threadIdx.x == 0) {
       r_finish(A, I, S, rmode, sm.res);
       A.counters[2 * t.inst] = 0;
@@ -594,10 +616,11 @@ __device__ void c_finish(const EngineArgs& A, const Inst& I, State* S, int cmode
 
 __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
   const Tile t = A.ctiles[ti];
-  const Inst& I = A.inst[t.inst];
   State* S = A.st + t.inst;
   const int cmode = ld_mut(&S->cmode);
   if (cmode == C_NONE) return;
+  const Inst& I = cache_inst(A, t.inst, sm);
+  const int cprimal = ld_mut(&S->cprimal);
 
   const int L = I.lanes_c;
   const int* __restrict__ cp = I.cp;
@@ -711,8 +734,9 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
     }
     case C_POWER: {
       const double* cx = I.cx;
-      tile_spmv<1>(t, cp, L, [&](int j, int p, double& a0, double&) {
-        a0 += ld_mut(cx + p) * ld_mut(I.ybar + ld_ro(ci + p));
+      const double* av = I.ybar;
+      tile_spmv<1>(t, cp, L, [&](int p, int) {
+        return ld_mut(cx + p) * ld_mut(av + ld_ro(ci + p));
       }, sm);
       for (int j = t.begin + threadIdx.x; j < rend; j += blockDim.x) {
         const double v = sm.s0[j - t.begin];
@@ -725,9 +749,10 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
       // backend.py:282-291 (aty += ady; sum_x += eta x) then the next primal step
       const double* cx = I.cx;
       const bool xc = ld_mut(&S->xcommit) != 0;
-      const int kind = ld_mut(&S->cprimal);
-      tile_spmv<1>(t, cp, L, [&](int j, int p, double& a0, double&) {
-        a0 += ld_mut(cx + p) * ld_mut(I.dy + ld_ro(ci + p));
+      const int kind = cprimal;
+      const double* dyv = I.dy;
+      tile_spmv<1>(t, cp, L, [&](int p, int) {
+        return ld_mut(cx + p) * ld_mut(dyv + ld_ro(ci + p));
       }, sm);
       for (int j = t.begin + threadIdx.x; j < rend; j += blockDim.x) {
         const double xv = xc ? ld_mut(I.xnew + j) : ld_mut(I.x + j);
@@ -743,7 +768,7 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
       break;
     }
     case C_PRIMAL: {
-      const int kind = ld_mut(&S->cprimal);
+      const int kind = cprimal;
       for (int j = t.begin + threadIdx.x; j < rend; j += blockDim.x)
         acc[0] += primal_half(I, j, ld_mut(I.x + j), ld_mut(I.aty + j), tau, kind, false);
       break;
@@ -769,11 +794,11 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
     }
     case C_CHECK_B: {
       const double* cx = I.cx;
-      tile_spmv<2>(t, cp, L, [&](int j, int p, double& a0, double& a1) {
+      const double* yb = I.ybar;
+      const double* yc = I.y;
+      tile_spmv<2>(t, cp, L, [&](int p, int rhs) {
         const int i = ld_ro(ci + p);
-        const double a = ld_mut(cx + p);
-        a0 += a * ld_mut(I.ybar + i);
-        a1 += a * ld_mut(I.y + i);
+        return ld_mut(cx + p) * ld_mut((rhs == 0 ? yb : yc) + i);
       }, sm);
       const double s = ld_mut(&S->s_obj);
       ops.maxmask = (1u << 0) | (1u << 2) | (1u << 3) | (1u << 4) | (1u << 6);
@@ -798,7 +823,7 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
     }
     case C_RESTART: {
       const bool avg = ld_mut(&S->restart_src) != 0;
-      const int kind = ld_mut(&S->cprimal);
+      const int kind = cprimal;
       for (int j = t.begin + threadIdx.x; j < rend; j += blockDim.x) {
         const double xv = avg ? ld_mut(I.xbar + j) : ld_mut(I.x + j);
         const double atyv = avg ? ld_mut(I.atybar + j) : ld_mut(I.atyf + j);
@@ -816,8 +841,8 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
       const bool avg = ld_mut(&S->final_src) != 0;
       const double* ysrc = avg ? I.ybar : I.y;
       const double* cx = I.cx;
-      tile_spmv<1>(t, cp, L, [&](int j, int p, double& a0, double&) {
-        a0 += ld_mut(cx + p) * ld_mut(ysrc + ld_ro(ci + p));
+      tile_spmv<1>(t, cp, L, [&](int p, int) {
+        return ld_mut(cx + p) * ld_mut(ysrc + ld_ro(ci + p));
       }, sm);
       const double s = ld_mut(&S->s_obj);
       const double dsign = I.sense == 1 ? 1.0 : -1.0;
@@ -834,15 +859,23 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
     default: break;
   }
 
-  block_reduce(acc, ops, sm);
-  if (threadIdx.x == 0) {
+  const bool trial = (cmode == C_ITER || cmode == C_PRIMAL || cmode == C_RESTART) &&
+                     cprimal == P_TRIAL;
+  const bool need_red = trial || cmode == C_RUIZ || cmode == C_APPLY || cmode == C_SETUP0 ||
+                        cmode == C_POWER || cmode == C_CHECK_A || cmode == C_CHECK_B ||
+                        cmode == C_FINAL;
+  if (need_red) {
+    block_reduce(acc, ops, sm);
+    if (threadIdx.x == 0) {
 #pragma unroll
-    for (int s = 0; s < kNP; ++s)
-      A.partials[(size_t)(A.n_rtiles + ti) * kNP + s] = sm.res[s];
+      for (int s = 0; s < kNP; ++s)
+        A.partials[(size_t)(A.n_rtiles + ti) * kNP + s] = sm.res[s];
+    }
   }
   const int ntiles = I.ct_end - I.ct_begin;
+  const int ct0 = I.ct_begin, ct1 = I.ct_end;
   if (finisher_enter(A.counters + 2 * t.inst + 1, ntiles, sm)) {
-    reduce_tiles(A.partials + (size_t)A.n_rtiles * kNP, I.ct_begin, I.ct_end, ops, sm);
+    if (need_red) reduce_tiles(A.partials + (size_t)A.n_rtiles * kNP, ct0, ct1, ops, sm);
     if (threadIdx.x == 0) {
       c_finish(A, I, S, cmode, sm.res);
       A.counters[2 * t.inst + 1] = 0;

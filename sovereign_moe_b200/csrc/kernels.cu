@@ -67,6 +67,7 @@ int launch_spmv(int m, const int64_t* rp, const int* ri, const T* rx, const T* x
     default: spmv_kernel<T, 32><<<g, kT, 0, st>>>(m, rp, ri, rx, x, y); break;
   }
   PDLP_CUDA(cudaGetLastError());
+  count_launches(1);
   return PDLP_OK;
 }
 
@@ -196,6 +197,7 @@ int reduce(long long n, const double* a, const double* b, int op, double* out, c
   PDLP_CUDA(cudaMallocAsync((void**)&scratch, sizeof(double) * (kRedBlocks + 1), st));
   reduce_partial_kernel<<<kRedBlocks, kT, 0, st>>>(n, a, b, op, scratch);
   reduce_final_kernel<<<1, kT, 0, st>>>(kRedBlocks, scratch, op, scratch + kRedBlocks);
+  count_launches(2);
   cudaError_t e = cudaGetLastError();
   double h = 0.0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h, scratch + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, st);
@@ -231,6 +233,7 @@ int pdlp_spmm_f64(int32_t m, int32_t k, const int64_t* rp, const int32_t* ri,
   const long long threads = (long long)m * k;
   spmm_kernel<<<grid_1d(threads), kT, 0, (cudaStream_t)stream>>>(m, k, rp, ri, rx, X, Y);
   PDLP_CUDA(cudaGetLastError());
+  count_launches(1);
   return PDLP_OK;
 }
 
@@ -241,6 +244,7 @@ int pdlp_primal_step(int32_t n, double* xnew, const double* x, const double* c,
   if (n == 0) return PDLP_OK;
   primal_step_kernel<<<grid_1d(n), kT, 0, (cudaStream_t)stream>>>(n, xnew, x, c, aty, lo, hi, tau);
   PDLP_CUDA(cudaGetLastError());
+  count_launches(1);
   return PDLP_OK;
 }
 
@@ -250,6 +254,7 @@ int pdlp_dual_step(int32_t m, double* ynew, const double* y, const double* ax,
   if (m == 0) return PDLP_OK;
   dual_step_kernel<<<grid_1d(m), kT, 0, (cudaStream_t)stream>>>(m, ynew, y, ax, rl, ru, sigma);
   PDLP_CUDA(cudaGetLastError());
+  count_launches(1);
   return PDLP_OK;
 }
 
@@ -259,6 +264,7 @@ int pdlp_pdhg_primal(int32_t n, double* x, double* dx, const double* c, const do
   if (n == 0) return PDLP_OK;
   pdhg_primal_kernel<<<grid_1d(n), kT, 0, (cudaStream_t)stream>>>(n, x, dx, c, aty, lo, hi, tau);
   PDLP_CUDA(cudaGetLastError());
+  count_launches(1);
   return PDLP_OK;
 }
 
@@ -268,6 +274,7 @@ int pdlp_pdhg_dual(int32_t m, double* y, double* dy, double* ax, const double* a
   if (m == 0) return PDLP_OK;
   pdhg_dual_kernel<<<grid_1d(m), kT, 0, (cudaStream_t)stream>>>(m, y, dy, ax, adx, rl, ru, sigma);
   PDLP_CUDA(cudaGetLastError());
+  count_launches(1);
   return PDLP_OK;
 }
 
@@ -277,6 +284,7 @@ int pdlp_pdhg_accum(int32_t n, double* acc, const double* inc, double* run_sum,
   if (n == 0) return PDLP_OK;
   pdhg_accum_kernel<<<grid_1d(n), kT, 0, (cudaStream_t)stream>>>(n, acc, inc, run_sum, v, eta);
   PDLP_CUDA(cudaGetLastError());
+  count_launches(1);
   return PDLP_OK;
 }
 

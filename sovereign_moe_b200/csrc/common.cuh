@@ -44,6 +44,21 @@ __device__ __forceinline__ long long ld_mut(const long long* p) { return __ldcg(
 __device__ __forceinline__ double ld_ro(const double* p) { return __ldg(p); }
 __device__ __forceinline__ int ld_ro(const int* p) { return __ldg(p); }
 
+// Acquire-release atomic add at GPU scope: publishes this thread's earlier
+// writes (and, through a preceding bar.sync, its block's) and, for the thread
+// that reads the final count, makes the other arrivers' writes visible.
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 __device__ __forceinline__ long long global_ns() {
   long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

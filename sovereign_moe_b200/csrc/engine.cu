@@ -18,23 +18,21 @@ namespace pdlp {
 // Arrive with a fenced atomic, wait for the generation to flip.  The wait is
 // bounded in wall time: on timeout the block records PDLP_ERR_BARRIER_TIMEOUT
 // in the control block and every block leaves the kernel at its next barrier.
-__device__ bool grid_barrier(Control* ctl, unsigned nblocks, long long timeout_ns, Smem& sm) {
+// Grid barrier on a monotonic arrival counter: the k-th barrier of a launch
+// is passed once the counter reaches k * nblocks (the host zeroes it before
+// each launch).  Arrival is an acquire-release add, the wait an acquire load,
+// so one atomic and one poll separate the last arrival from the release of
+// every block.  The wait is bounded in wall time: on timeout the block
+// records PDLP_ERR_BARRIER_TIMEOUT and every block leaves the kernel.
+__device__ bool grid_barrier(Control* ctl, unsigned target, long long timeout_ns, int* flag) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* gen = &ctl->bar_gen;
     volatile int* err = &ctl->error;
-    const unsigned g = *gen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(&ctl->bar_count, 1u) + 1u;
     int ok = 1;
-    if (arrived == nblocks) {
-      atomicExch(&ctl->bar_count, 0u);
-      __threadfence();
-      atomicAdd((unsigned*)&ctl->bar_gen, 1u);
-    } else {
+    if (atom_add_acq_rel(&ctl->bar_count, 1u) + 1u < target) {
       const long long t0 = global_ns();
       unsigned spins = 0;
-      while (*gen == g) {
+      while (ld_acquire(&ctl->bar_count) < target) {
         if ((++spins & 255u) == 0u) {
           if (*err != 0) { ok = 0; break; }
           if (global_ns() - t0 > timeout_ns) {
@@ -45,44 +43,88 @@ __device__ bool grid_barrier(Control* ctl, unsigned nblocks, long long timeout_n
         }
       }
     }
-    __threadfence();
-    sm.flag = ok && (*err == 0);
+    *flag = ok && (*err == 0);
   }
   __syncthreads();
-  return sm.flag != 0;
+  return *flag != 0;
 }
 
+// One launch runs up to max_steps engine steps; every warp owns a fixed range
+// of row tiles and of column tiles for the whole launch.
 extern __shared__ __align__(16) unsigned char g_smem[];
+constexpr size_t kSmemBytes = sizeof(WarpSmem) * kWarps + 16;
 
-__global__ void __launch_bounds__(kBlock) engine_persistent(EngineArgs A) {
-  Smem& sm = *reinterpret_cast<Smem*>(g_smem);
-  if (threadIdx.x == 0) sm.inst_id = -1;
-  __syncthreads();
+__global__ void __launch_bounds__(kBlock, 3) engine_persistent(EngineArgs A) {
+  WarpSmem* ws = reinterpret_cast<WarpSmem*>(g_smem);
+  int& flag = *reinterpret_cast<int*>(g_smem + sizeof(WarpSmem) * kWarps);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpSmem& W = ws[warp];
+  if (lane == 0) W.inst_id = -1;
+  __syncwarp();
   const unsigned nb = gridDim.x;
-  const int b = blockIdx.x;
-  const int r0 = A.rblock[b], r1 = A.rblock[b + 1];
-  const int c0 = A.cblock[b], c1 = A.cblock[b + 1];
+  const int gw = blockIdx.x * kWarps + warp;
+  const int r0 = A.rwarp[gw], r1 = A.rwarp[gw + 1];
+  const int c0 = A.cwarp[gw], c1 = A.cwarp[gw + 1];
+  // the warp's first tile of each side stays in registers for the launch
+  const Tile rfirst = r0 < r1 ? A.rtiles[r0] : Tile{};
+  const Tile cfirst = c0 < c1 ? A.ctiles[c0] : Tile{};
+  unsigned target = 0;
+#ifdef PDLP_TRACE
+  // phase timestamps of the first and the last block for the first steps
+  long long* tr = nullptr;
+  if (A.trace && threadIdx.x == 0 && (blockIdx.x == 0 || blockIdx.x == gridDim.x - 1))
+    tr = A.trace + (blockIdx.x == 0 ? 0 : 64 * 5);
+#define PDLP_STAMP(step, k) if (tr && (step) < 64) tr[(step) * 5 + (k)] = global_ns()
+#else
+#define PDLP_STAMP(step, k)
+#endif
   for (long long step = 0; step < A.max_steps; ++step) {
-    if (threadIdx.x == 0) sm.flag = *(volatile int*)&A.ctl->active;
+    if (threadIdx.x == 0) flag = *(volatile int*)&A.ctl->active;
     __syncthreads();
-    if (sm.flag <= 0) return;
+    if (flag <= 0) return;
     __syncthreads();
-    for (int t = r0; t < r1; ++t) process_rtile(A, t, sm);
-    if (!grid_barrier(A.ctl, nb, A.barrier_timeout_ns, sm)) return;
-    for (int t = c0; t < c1; ++t) process_ctile(A, t, sm);
-    if (!grid_barrier(A.ctl, nb, A.barrier_timeout_ns, sm)) return;
+    PDLP_STAMP(step, 0);
+    {
+      Tile next = rfirst;
+      for (int t = r0; t < r1; ++t) {
+        const Tile cur = next;
+        if (t + 1 < r1) next = A.rtiles[t + 1];      // prefetch the next descriptor
+        process_rtile(A, cur, t, W, lane);
+      }
+    }
+    PDLP_STAMP(step, 1);
+    target += nb;
+    if (!grid_barrier(A.ctl, target, A.barrier_timeout_ns, &flag)) return;
+    PDLP_STAMP(step, 2);
+    {
+      Tile next = cfirst;
+      for (int t = c0; t < c1; ++t) {
+        const Tile cur = next;
+        if (t + 1 < c1) next = A.ctiles[t + 1];
+        process_ctile(A, cur, t, W, lane);
+      }
+    }
+    PDLP_STAMP(step, 3);
+    target += nb;
+    if (!grid_barrier(A.ctl, target, A.barrier_timeout_ns, &flag)) return;
+    PDLP_STAMP(step, 4);
   }
+#undef PDLP_STAMP
 }
 
 // One pass over all tiles of one side; kernel boundaries are the barriers.
-__global__ void __launch_bounds__(kBlock) engine_pass(EngineArgs A, int side) {
-  Smem& sm = *reinterpret_cast<Smem*>(g_smem);
-  if (threadIdx.x == 0) sm.inst_id = -1;
-  __syncthreads();
+__global__ void __launch_bounds__(kBlock, 3) engine_pass(EngineArgs A, int side) {
+  WarpSmem* ws = reinterpret_cast<WarpSmem*>(g_smem);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpSmem& W = ws[warp];
+  if (lane == 0) W.inst_id = -1;
+  __syncwarp();
+  const int gw = blockIdx.x * kWarps + warp;
+  const int nw = gridDim.x * kWarps;
   if (side == 0) {
-    for (int t = blockIdx.x; t < A.n_rtiles; t += gridDim.x) process_rtile(A, t, sm);
+    for (int t = gw; t < A.n_rtiles; t += nw) process_rtile(A, A.rtiles[t], t, W, lane);
   } else {
-    for (int t = blockIdx.x; t < A.n_ctiles; t += gridDim.x) process_ctile(A, t, sm);
+    for (int t = gw; t < A.n_ctiles; t += nw) process_ctile(A, A.ctiles[t], t, W, lane);
   }
 }
 
@@ -131,16 +173,18 @@ constexpr size_t kAlign = 256;
 
 size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
-int default_tile_rows() { return 512; }
-int default_tile_nnz() { return kTileNnz; }
-int heavy_threshold() { return kTileNnz; }   // longer rows: a block-wide tile alone
+int default_tile_rows() { return kWTileRows; }
+int default_tile_nnz() { return kWTileNnz; }
+int heavy_threshold() { return kWTileNnz; }  // longer rows: a warp-wide tile alone
 
+// Lanes per row for the row sums of an LP side.  The products are already
+// in shared memory, so a lane summing its row alone (in storage order) beats
+// splitting the row across lanes, whose shuffle tree is a serial chain; only
+// long rows get 2 or 4 lanes.
 int lanes_for(long long nnz, long long rows) {
   if (rows <= 0) return 1;
-  double avg = (double)nnz / (double)rows;
-  int L = 1;
-  while (L < 32 && L < avg) L <<= 1;
-  return L;
+  const double avg = (double)nnz / (double)rows;
+  return avg <= 48.0 ? 1 : (avg <= 160.0 ? 2 : 4);
 }
 
 // Split the rows of one side into tiles of at most `rows_cap` rows and about
@@ -154,21 +198,21 @@ void plan_tiles(const int64_t* ptr, int nrows, int inst, int rows_cap, int nnz_c
   for (int r = 0; r < nrows; ++r) {
     long long len = ptr[r + 1] - ptr[r];
     if (len > heavy) {
-      if (r > b) out.push_back({inst, b, r, 0});
-      out.push_back({inst, r, r + 1, 1});
+      if (r > b) out.push_back({inst, b, r, 0, 0, (int)ptr[b], (int)(ptr[r] - ptr[b]), 0});
+      out.push_back({inst, r, r + 1, 1, 0, (int)ptr[r], (int)len, 0});
       b = r + 1;
       acc = 0;
       continue;
     }
     if (r > b && (r - b >= rows_cap || acc + len > nnz_cap)) {
-      out.push_back({inst, b, r, 0});
+      out.push_back({inst, b, r, 0, 0, (int)ptr[b], (int)(ptr[r] - ptr[b]), 0});
       b = r;
       acc = 0;
     }
     acc += len;
   }
-  if (nrows > b) out.push_back({inst, b, nrows, 0});
-  if (nrows == 0) out.push_back({inst, 0, 0, 0});   // the pass still finishes
+  if (nrows > b) out.push_back({inst, b, nrows, 0, 0, (int)ptr[b], (int)(ptr[nrows] - ptr[b]), 0});
+  if (nrows == 0) out.push_back({inst, 0, 0, 0, 0, 0, 0, 0});   // the pass still finishes
   // work estimate per tile: entries (value + index + gather) and rows (vectors)
   for (size_t i = first; i < out.size(); ++i) {
     const Tile& t = out[i];
@@ -204,10 +248,15 @@ struct pdlp_batch {
   Control* d_ctl = nullptr;
   Tile* d_rtiles = nullptr;
   Tile* d_ctiles = nullptr;
-  int* d_rblock = nullptr;
-  int* d_cblock = nullptr;
+  int* d_rwarp = nullptr;
+  int* d_cwarp = nullptr;
+  int2* d_group_tiles = nullptr;
   double* d_partials = nullptr;
-  size_t cap_rtiles = 0, cap_ctiles = 0, cap_blocks = 0, cap_partials = 0;
+  double* d_gpartials = nullptr;
+  unsigned* d_gcounters = nullptr;
+  size_t cap_rtiles = 0, cap_ctiles = 0, cap_rwarp = 0, cap_cwarp = 0, cap_partials = 0;
+  size_t cap_groups = 0, cap_gpartials = 0, cap_gcounters = 0;
+  int n_rgroups = 0, n_groups = 0;
   int n_rtiles = 0, n_ctiles = 0, grid = 0;
   bool dirty = true;
   bool broken = false;
@@ -282,6 +331,7 @@ SlotLayout layout_for(int m, int n, long long nnz, bool kind, bool v0, int hist_
   for (int i = 0; i < 14; ++i) s.mvec[i] = L.take(sizeof(double) * (size_t)m);
   for (int i = 0; i < 16; ++i) s.nvec[i] = L.take(sizeof(double) * (size_t)n);
   s.hist = L.take(sizeof(double) * 5 * (size_t)std::max(hist_cap, 0));
+  L.take(256);     // 16-byte staging copies may read a few bytes past the last array
   s.total = L.off;
   return s;
 }
@@ -314,6 +364,18 @@ void block_ranges(const std::vector<double>& w, int G, std::vector<int>& out) {
 
 }  // namespace
 
+// Group the tiles of one instance-side into reduction groups of kGroupTiles
+// consecutive tiles; appends (tile range) per group and stamps each tile.
+static void make_groups(std::vector<Tile>& tiles, int t0, int t1, int group_base,
+                        std::vector<int2>& groups) {
+  for (int g0 = t0; g0 < t1; g0 += kGroupTiles) {
+    const int g1 = std::min(t1, g0 + kGroupTiles);
+    const int gid = group_base + (int)groups.size();
+    for (int t = g0; t < g1; ++t) tiles[t].group = gid;
+    groups.push_back(make_int2(g0, g1));
+  }
+}
+
 static int rebuild(pdlp_batch* b) {
   std::vector<Tile> rt, ct;
   std::vector<double> rw, cw;
@@ -329,32 +391,59 @@ static int rebuild(pdlp_batch* b) {
     cw.insert(cw.end(), sl.ctw.begin(), sl.ctw.end());
     sl.inst.ct_end = (int)ct.size();
   }
+  // reduction groups: row-side groups first, then column-side groups
+  std::vector<int2> rgroups, cgroups;
+  for (size_t s = 0; s < b->slots.size(); ++s) {
+    Slot& sl = b->slots[s];
+    if (!sl.used || !sl.running) continue;
+    sl.inst.rg_begin = (int)rgroups.size();
+    make_groups(rt, sl.inst.rt_begin, sl.inst.rt_end, 0, rgroups);
+    sl.inst.rg_end = (int)rgroups.size();
+  }
+  const int nrg = (int)rgroups.size();
+  for (size_t s = 0; s < b->slots.size(); ++s) {
+    Slot& sl = b->slots[s];
+    if (!sl.used || !sl.running) continue;
+    sl.inst.cg_begin = nrg + (int)cgroups.size();
+    make_groups(ct, sl.inst.ct_begin, sl.inst.ct_end, nrg, cgroups);
+    sl.inst.cg_end = nrg + (int)cgroups.size();
+  }
+  std::vector<int2> groups(rgroups);
+  groups.insert(groups.end(), cgroups.begin(), cgroups.end());
+  b->n_rgroups = nrg;
+  b->n_groups = (int)groups.size();
   b->n_rtiles = (int)rt.size();
   b->n_ctiles = (int)ct.size();
-  int G = std::max(1, std::min(b->sms * b->coop_blocks_per_sm,
-                               std::max(b->n_rtiles, b->n_ctiles)));
+  // persistent grid: enough warps for the larger tile list, at most what is co-resident
+  const int max_blocks = std::max(1, b->sms * b->coop_blocks_per_sm);
+  const int want = (std::max(b->n_rtiles, b->n_ctiles) + kWarps - 1) / kWarps;
+  const int G = std::max(1, std::min(max_blocks, want));
   b->grid = G;
-  std::vector<int> rb, cb;
-  block_ranges(rw, G, rb);
-  block_ranges(cw, G, cb);
+  std::vector<int> rwr, cwr;
+  block_ranges(rw, G * kWarps, rwr);
+  block_ranges(cw, G * kWarps, cwr);
   int rc;
   if ((rc = ensure_capacity((void**)&b->d_rtiles, &b->cap_rtiles, rt.size(), sizeof(Tile)))) return rc;
   if ((rc = ensure_capacity((void**)&b->d_ctiles, &b->cap_ctiles, ct.size(), sizeof(Tile)))) return rc;
-  size_t need_blocks = (size_t)G + 1;
-  if (need_blocks > b->cap_blocks || !b->d_rblock) {
-    size_t cap = b->cap_blocks;
-    if ((rc = ensure_capacity((void**)&b->d_rblock, &cap, need_blocks, sizeof(int)))) return rc;
-    cap = b->cap_blocks;
-    if ((rc = ensure_capacity((void**)&b->d_cblock, &cap, need_blocks, sizeof(int)))) return rc;
-    b->cap_blocks = cap;
-  }
+  if ((rc = ensure_capacity((void**)&b->d_rwarp, &b->cap_rwarp, rwr.size(), sizeof(int)))) return rc;
+  if ((rc = ensure_capacity((void**)&b->d_cwarp, &b->cap_cwarp, cwr.size(), sizeof(int)))) return rc;
   if ((rc = ensure_capacity((void**)&b->d_partials, &b->cap_partials,
                             (rt.size() + ct.size()) * kNP, sizeof(double)))) return rc;
+  if ((rc = ensure_capacity((void**)&b->d_group_tiles, &b->cap_groups, groups.size(), sizeof(int2)))) return rc;
+  if ((rc = ensure_capacity((void**)&b->d_gpartials, &b->cap_gpartials, groups.size() * kNP,
+                            sizeof(double)))) return rc;
+  if ((rc = ensure_capacity((void**)&b->d_gcounters, &b->cap_gcounters, groups.size(),
+                            sizeof(unsigned)))) return rc;
   cudaStream_t st = b->stream;
   if (!rt.empty()) PDLP_CUDA(cudaMemcpyAsync(b->d_rtiles, rt.data(), rt.size() * sizeof(Tile), cudaMemcpyHostToDevice, st));
   if (!ct.empty()) PDLP_CUDA(cudaMemcpyAsync(b->d_ctiles, ct.data(), ct.size() * sizeof(Tile), cudaMemcpyHostToDevice, st));
-  PDLP_CUDA(cudaMemcpyAsync(b->d_rblock, rb.data(), rb.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-  PDLP_CUDA(cudaMemcpyAsync(b->d_cblock, cb.data(), cb.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  PDLP_CUDA(cudaMemcpyAsync(b->d_rwarp, rwr.data(), rwr.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  PDLP_CUDA(cudaMemcpyAsync(b->d_cwarp, cwr.data(), cwr.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  if (!groups.empty())
+    PDLP_CUDA(cudaMemcpyAsync(b->d_group_tiles, groups.data(), groups.size() * sizeof(int2),
+                              cudaMemcpyHostToDevice, st));
+  PDLP_CUDA(cudaMemsetAsync(b->d_gcounters, 0, groups.size() * sizeof(unsigned), st));
+  PDLP_CUDA(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2 * b->slots.size(), st));
   std::vector<Inst> insts(b->slots.size());
   for (size_t s = 0; s < b->slots.size(); ++s) insts[s] = b->slots[s].inst;
   PDLP_CUDA(cudaMemcpyAsync(b->d_inst, insts.data(), insts.size() * sizeof(Inst), cudaMemcpyHostToDevice, st));
@@ -416,9 +505,9 @@ int pdlp_batch_create(const pdlp_batch_config* cfg, void* stream, pdlp_batch** o
   if (c.block_threads == 0) c.block_threads = kBlock;
   if (c.block_threads != kBlock) return fail(PDLP_ERR_ARG, "block_threads must be 256");
   if (c.tile_rows <= 0) c.tile_rows = default_tile_rows();
-  if (c.tile_rows > kMaxTileRows) return fail(PDLP_ERR_ARG, "tile_rows exceeds 1024");
+  if (c.tile_rows > kWTileRows) return fail(PDLP_ERR_ARG, "tile_rows exceeds 128");
   if (c.tile_nnz <= 0) c.tile_nnz = default_tile_nnz();
-  if (c.tile_nnz > kTileNnz) return fail(PDLP_ERR_ARG, "tile_nnz exceeds 4096");
+  if (c.tile_nnz > kWTileNnz) return fail(PDLP_ERR_ARG, "tile_nnz exceeds 512");
   if (c.lanes_override && (c.lanes_override & (c.lanes_override - 1)))
     return fail(PDLP_ERR_ARG, "lanes_override must be a power of two");
   pdlp_batch* b = new pdlp_batch();
@@ -438,13 +527,13 @@ int pdlp_batch_create(const pdlp_batch_config* cfg, void* stream, pdlp_batch** o
   int coop = 0;
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
   if ((e = cudaFuncSetAttribute(engine_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sizeof(Smem))) != cudaSuccess)
+                                (int)kSmemBytes)) != cudaSuccess)
     return bail(e, "cudaFuncSetAttribute");
   if ((e = cudaFuncSetAttribute(engine_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sizeof(Smem))) != cudaSuccess)
+                                (int)kSmemBytes)) != cudaSuccess)
     return bail(e, "cudaFuncSetAttribute");
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->coop_blocks_per_sm, engine_persistent,
-                                                          kBlock, sizeof(Smem))) != cudaSuccess)
+                                                          kBlock, kSmemBytes)) != cudaSuccess)
     return bail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
   if (!coop || b->coop_blocks_per_sm < 1) b->cfg.persistent = 0;
   if ((e = cudaMalloc(&b->d_inst, sizeof(Inst) * c.max_slots)) != cudaSuccess) return bail(e, "cudaMalloc");
@@ -471,8 +560,9 @@ int pdlp_batch_destroy(pdlp_batch* b) {
   cudaStreamSynchronize(b->stream);
   for (auto& s : b->slots) if (s.arena) cudaFree(s.arena);
   cudaFree(b->d_inst); cudaFree(b->d_state); cudaFree(b->d_counters); cudaFree(b->d_ctl);
-  cudaFree(b->d_rtiles); cudaFree(b->d_ctiles); cudaFree(b->d_rblock); cudaFree(b->d_cblock);
-  cudaFree(b->d_partials);
+  cudaFree(b->d_rtiles); cudaFree(b->d_ctiles); cudaFree(b->d_rwarp); cudaFree(b->d_cwarp);
+  cudaFree(b->d_partials); cudaFree(b->d_group_tiles); cudaFree(b->d_gpartials);
+  cudaFree(b->d_gcounters);
   if (b->h_ctl) cudaFreeHost(b->h_ctl);
   if (b->h_state) cudaFreeHost(b->h_state);
   if (b->ev0) cudaEventDestroy(b->ev0);
@@ -661,6 +751,13 @@ int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out) {
   int rc;
   cudaStream_t st = b->stream;
   EngineArgs A{};
+  A.trace = nullptr;
+#ifdef PDLP_TRACE
+  static long long* d_trace = nullptr;
+  if (!d_trace) { cudaMalloc(&d_trace, sizeof(long long) * 1280); }
+  cudaMemsetAsync(d_trace, 0, sizeof(long long) * 1280, b->stream);
+  A.trace = d_trace;
+#endif
   A.inst = b->d_inst; A.st = b->d_state;
   A.counters = b->d_counters; A.ctl = b->d_ctl;
   A.barrier_timeout_ns = 4000000000LL;
@@ -674,8 +771,9 @@ int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out) {
     if (b->dirty && (rc = rebuild(b))) return rc;
     A.rtiles = b->d_rtiles; A.n_rtiles = b->n_rtiles;
     A.ctiles = b->d_ctiles; A.n_ctiles = b->n_ctiles;
-    A.rblock = b->d_rblock; A.cblock = b->d_cblock;
-    A.partials = b->d_partials;
+    A.rwarp = b->d_rwarp; A.cwarp = b->d_cwarp;
+    A.group_tiles = b->d_group_tiles; A.n_rgroups = b->n_rgroups; A.n_groups = b->n_groups;
+    A.partials = b->d_partials; A.gpartials = b->d_gpartials; A.gcounters = b->d_gcounters;
     const int64_t chunk = std::min(left, kChunk);
     left -= chunk;
     A.max_steps = chunk;
@@ -686,14 +784,15 @@ int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out) {
     if (b->cfg.persistent) {
       void* args[] = {&A};
       PDLP_CUDA(cudaLaunchCooperativeKernel((void*)engine_persistent, dim3(b->grid), dim3(kBlock),
-                                            args, sizeof(Smem), st));
+                                            args, kSmemBytes, st));
       count_launches(1);
     } else {
-      const int g_r = std::max(1, std::min(b->n_rtiles, b->sms * b->coop_blocks_per_sm));
-      const int g_c = std::max(1, std::min(b->n_ctiles, b->sms * b->coop_blocks_per_sm));
+      const int cap = b->sms * b->coop_blocks_per_sm;
+      const int g_r = std::max(1, std::min((b->n_rtiles + kWarps - 1) / kWarps, cap));
+      const int g_c = std::max(1, std::min((b->n_ctiles + kWarps - 1) / kWarps, cap));
       for (int64_t s = 0; s < chunk; ++s) {
-        engine_pass<<<g_r, kBlock, sizeof(Smem), st>>>(A, 0);
-        engine_pass<<<g_c, kBlock, sizeof(Smem), st>>>(A, 1);
+        engine_pass<<<g_r, kBlock, kSmemBytes, st>>>(A, 0);
+        engine_pass<<<g_c, kBlock, kSmemBytes, st>>>(A, 1);
       }
       count_launches(2 * chunk);
       PDLP_CUDA(cudaGetLastError());
@@ -706,6 +805,38 @@ int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
     total_ms += ms;
+#ifdef PDLP_TRACE
+    {
+      long long h[1280];
+      cudaMemcpy(h, A.trace, sizeof(h), cudaMemcpyDeviceToHost);
+      {
+        double acc[7] = {0};
+        int cnt = 0;
+        for (int q = 1; q < 63; ++q) {
+          const long long* r = h + 640 + q * 8;
+          if (!r[6] || !r[7]) continue;
+          acc[0] += (r[0] - r[7]) * 1e-3;           // tile start -> hot path entry (state loads)
+          for (int k = 1; k < 7; ++k) acc[k] += (r[k] - r[k - 1]) * 1e-3;
+          ++cnt;
+        }
+        if (cnt) fprintf(stderr, "[trace] R hot tile (n=%d): pre=%.2f stage_issue=%.2f wait_matrix=%.2f gather=%.2f rowsum=%.2f wait_vec=%.2f epilogue=%.2f us\n",
+                         cnt, acc[0] / cnt, acc[1] / cnt, acc[2] / cnt, acc[3] / cnt, acc[4] / cnt, acc[5] / cnt, acc[6] / cnt);
+      }
+      for (int blk = 0; blk < 2; ++blk) {
+        double acc[4] = {0, 0, 0, 0};
+        int cnt = 0;
+        for (int st2 = 1; st2 < 64; ++st2) {
+          const long long* r = h + blk * 320 + st2 * 5;
+          if (!r[4]) break;
+          for (int k = 0; k < 4; ++k) acc[k] += (r[k + 1] - r[k]) * 1e-3;
+          ++cnt;
+        }
+        if (cnt) fprintf(stderr, "[trace] grid=%d block%s: steps=%d  Rtiles=%.2fus bar1=%.2fus Ctiles=%.2fus bar2=%.2fus\n",
+                         b->grid, blk ? "last" : "0", cnt, acc[0] / cnt, acc[1] / cnt, acc[2] / cnt, acc[3] / cnt);
+      }
+      cudaMemsetAsync(A.trace, 0, sizeof(long long) * 1280, st);
+    }
+#endif
     if (b->h_ctl->error) {
       b->broken = true;
       return fail(b->h_ctl->error, "engine: a bounded grid barrier timed out; the batch was stopped");

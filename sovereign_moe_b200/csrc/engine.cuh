@@ -9,10 +9,13 @@
 // depend on which other LPs share the launch.
 //
 // Every engine step runs the A pass over all row tiles, a grid-wide barrier,
-// the A^T pass over all column tiles and another barrier.  What a tile does
-// in a pass is set by its instance's state machine (RMode / CMode below); the
-// block that finishes an instance's last tile of a pass reduces that pass's
-// tile partials and advances the state machine (the "finisher").
+// the A^T pass over all column tiles and another barrier.  A tile is the work
+// of one warp (a few hundred entries); warps never wait for one another
+// inside a pass.  What a tile does is set by its instance's state machine
+// (RMode / CMode below).  Per-instance reductions go through a fixed two-level
+// tree: tile partials -> group partials (64 consecutive tiles) -> instance;
+// the warp that completes a group reduces it, and the warp that completes the
+// instance's last group advances the state machine (the "finisher").
 #pragma once
 
 #include <cstdint>
@@ -93,8 +96,9 @@ struct Inst {
   double time_limit_ns, time_used_ns;
   int check_every, stepsize_every;
   double beta_s, beta_n, beta_a, theta;
-  // tile ranges in the launch's tile lists
+  // tile and group ranges in the launch's lists
   int rt_begin, rt_end, ct_begin, ct_end;
+  int rg_begin, rg_end, cg_begin, cg_end;
 };
 
 // Mutable; written only by the instance's finishers (and by the host between
@@ -133,8 +137,13 @@ struct State {
 struct Tile {
   int inst;
   int begin, end;           // local row range
-  int heavy;                // 1: a single long row, reduced by the whole block
+  int heavy;                // 1: a single long row, reduced by the whole warp
+  int group;                // global index of the tile's reduction group
+  int p0, cnt;              // first entry and entry count of the row range
+  int pad;
 };
+
+constexpr int kGroupTiles = 64;          // tiles per reduction group
 
 // Engine-wide control block in device memory.
 struct Control {
@@ -151,14 +160,19 @@ struct EngineArgs {
   State* st;
   const Tile* rtiles; int n_rtiles;
   const Tile* ctiles; int n_ctiles;
-  const int* rblock;        // persistent: block b owns row tiles [rblock[b], rblock[b+1])
-  const int* cblock;
-  double* partials;         // [(n_rtiles + n_ctiles) * kNP]
-  unsigned int* counters;   // [2 * n_inst]
+  const int* rwarp;         // persistent: warp w owns row tiles [rwarp[w], rwarp[w+1])
+  const int* cwarp;
+  const int2* group_tiles;  // [n_groups]: tile range of each group (row groups first)
+  int n_rgroups, n_groups;
+  double* partials;         // [(n_rtiles + n_ctiles) * kNP] tile partials
+  double* gpartials;        // [n_groups * kNP] group partials
+  unsigned int* gcounters;  // [n_groups] tiles done per group
+  unsigned int* counters;   // [2 * n_inst] groups done per instance and side
   Control* ctl;
   long long max_steps;
   long long barrier_timeout_ns;
   int n_inst;
+  long long* trace;         // tracing builds only: phase timestamps, else null
 };
 
 }  // namespace pdlp

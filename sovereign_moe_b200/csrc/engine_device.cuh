@@ -1,11 +1,12 @@
-// Device code of the PDLP engine: tile passes, finishers, grid barrier.
+// Device helpers of the PDLP engine: warp-level tile passes and reductions.
 //
 // Algorithm: restarted averaged PDHG of src/sovopt/lp/pdlp.py:238-494 with
 // the method="pdlp" preconditioner of src/sovopt/numerics/scaling.py:149-478,
 // executed as a per-LP state machine (see engine.cuh).  Every arithmetic
 // expression of the reference's iteration is kept (same operands, same
-// order), in float64; sums over rows/columns use a fixed reduction tree, so a
-// run is bitwise repeatable and independent of the other LPs in the batch.
+// order), in float64.  Every sum uses an order that depends only on the LP
+// (its rows and the lanes-per-row choice), never on the batch, so a run is
+// bitwise repeatable and independent of the other LPs that share a launch.
 #pragma once
 
 #include "common.cuh"
@@ -13,24 +14,54 @@
 
 namespace pdlp {
 
-constexpr int kBlock = 256;            // threads per block (all engine kernels)
-constexpr int kMaxTileRows = 1024;     // rows per tile (shared-memory staging)
-constexpr int kTileNnz = 4096;         // entries per normal tile (products staged in smem)
+constexpr int kWarps = 4;              // warps per block (engine kernels)
+constexpr int kBlock = 32 * kWarps;    // threads per block
+constexpr int kWTileRows = 128;        // rows per normal tile
+constexpr int kWTileNnz = 512;         // entries per normal tile
+constexpr int kVecs = 7;               // vectors staged for a hot-mode epilogue
 constexpr double kRuizTol = 1e-2;      // scaling.py:149
 constexpr unsigned kFull = 0xffffffffu;
 
-// Per-block shared memory (dynamic: larger than the 48 KB static limit).
-struct Smem {
-  double prod[kTileNnz];               // products of the tile's entries
-  double s0[kMaxTileRows];             // row sums, first right-hand side
-  double s1[kMaxTileRows];             // row sums, second right-hand side
-  int ptr[kMaxTileRows + 1];           // the tile's row pointers
-  double red[32 * kNP];
-  double res[kNP];
-  Inst inst;                           // cached descriptor of inst_id
+// Per-warp shared memory.  The s* arrays receive 16-byte asynchronous copies
+// of a tile's row pointers, indices, values and epilogue vectors; each has
+// room for the alignment offset of the copied range.  sval doubles as the
+// products' staging area.
+struct __align__(16) WarpSmem {
+  int sptr[kWTileRows + 8];
+  int sidx[kWTileNnz + 8];
+  double sval[kWTileNnz + 4];
+  double vec[kVecs][kWTileRows + 4];
+  double s0[kWTileRows];               // row sums, first right-hand side
+  double s1[kWTileRows];               // row sums, second right-hand side
   int inst_id;
-  int flag;
+  int pad[3];
+  Inst inst;                           // cached descriptor of inst_id
 };
+
+// ---- asynchronous staging (cp.async, 16-byte, L2 only) -----------------------
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Stage elements [first, first + count) of a 16-byte-aligned array of
+// E-byte elements into dst in whole 16-byte chunks; returns the index in dst
+// of element `first`.  The last chunk may read up to 12 bytes past the range
+// (every array of a slot's arena is followed by padding).
+template <int E>
+__device__ __forceinline__ int stage(void* dst, const void* base, int first, int count, int lane) {
+  constexpr int per = 16 / E;
+  const int a = first & ~(per - 1);
+  const int nchunks = (first + count - a + per - 1) / per;
+  const char* src = reinterpret_cast<const char*>(base) + (size_t)a * E;
+  char* d = reinterpret_cast<char*>(dst);
+  for (int c = lane; c < nchunks; c += 32) cp_async16(d + 16 * c, src + 16 * c);
+  return first - a;
+}
 
 // ---- reductions -----------------------------------------------------------
 
@@ -51,199 +82,160 @@ struct Ops {
   }
 };
 
-// Block-wide reduction of kNP slots; the result lands in sm.res (all threads
-// may read it after the call).  Fixed shuffle tree: deterministic.
-__device__ void block_reduce(double* v, Ops ops, Smem& sm) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nwarps = blockDim.x >> 5;
+// Warp-wide reduction of kNP slots with a fixed xor tree; every lane ends
+// with the result.
+__device__ __forceinline__ void warp_reduce(double* v, Ops ops) {
 #pragma unroll
   for (int s = 0; s < kNP; ++s) {
-    int op = ops.op(s);
-    double a = v[s];
+    const int op = ops.op(s);
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) a = combine(a, __shfl_down_sync(kFull, a, off), op);
-    if (lane == 0) sm.red[warp * kNP + s] = a;
+    for (int off = 16; off > 0; off >>= 1) v[s] = combine(v[s], __shfl_xor_sync(kFull, v[s], off), op);
   }
-  __syncthreads();
-  if (warp == 0) {
-#pragma unroll
-    for (int s = 0; s < kNP; ++s) {
-      int op = ops.op(s);
-      double a = lane < nwarps ? sm.red[lane * kNP + s] : identity_of(op);
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) a = combine(a, __shfl_down_sync(kFull, a, off), op);
-      if (lane == 0) sm.res[s] = a;
-    }
-  }
-  __syncthreads();
 }
 
-// ---- sparse row passes ----------------------------------------------------
+// ---- sparse passes over one tile (one warp) ---------------------------------
 
-// out[r - b] = sum over row r of term(r, p), rows [b, e), L lanes per row.
-// Each lane sums its strided entries in storage order, then a xor butterfly
-// combines the L lanes; with L == 1 the sum is fully sequential.
+// Row sums of the tile for NR right-hand sides into W.s0 (W.s1).
+// Normal tile: every entry's product is computed first -- all loads and
+// gathers of the tile independent of each other -- and staged in shared
+// memory; each row is then summed by L lanes (each lane its strided entries in
+// storage order, then a xor butterfly; L == 1 is the storage-order sum).
+// Heavy tile (one row longer than a normal tile holds): the 32 lanes stride
+// over the row, then a xor butterfly.  Either way the order depends only on
+// the row and L.  term(p, rhs) returns value[p] * x_rhs[index[p]].
 template <int NR, class F>
-__device__ __forceinline__ void rows_spmv(const int* __restrict__ ptr, int b, int e, int L,
-                                          F f, double* s0, double* s1) {
-  const int tid = threadIdx.x;
-  const int lane = tid & (L - 1);
-  const int grp = tid / L, ngrp = blockDim.x / L;
-  for (int rb = b; rb < e; rb += ngrp) {
-    const int r = rb + grp;
+__device__ __forceinline__ void warp_spmv(const Tile& t, const int* ptr, const int* tptr, int L,
+                                          F term, WarpSmem& W, int lane) {
+  if (t.heavy) {
+    const int p0 = ld_ro(ptr + t.begin), p1 = ld_ro(ptr + t.begin + 1);
     double a0 = 0.0, a1 = 0.0;
-    if (r < e) {
-      const int p0 = ld_ro(ptr + r), p1 = ld_ro(ptr + r + 1);
-      for (int p = p0 + lane; p < p1; p += L) f(r, p, a0, a1);
+    for (int p = p0 + lane; p < p1; p += 32) {
+      a0 += term(p, 0);
+      if (NR == 2) a1 += term(p, 1);
     }
-    for (int off = L >> 1; off > 0; off >>= 1) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
       a0 += __shfl_xor_sync(kFull, a0, off);
       if (NR == 2) a1 += __shfl_xor_sync(kFull, a1, off);
     }
-    if (r < e && lane == 0) {
-      s0[r - b] = a0;
-      if (NR == 2) s1[r - b] = a1;
-    }
+    if (lane == 0) { W.s0[0] = a0; if (NR == 2) W.s1[0] = a1; }
+    __syncwarp();
+    return;
   }
-}
-
-// One long row reduced by the whole block (fixed tree); result in s0[0], s1[0].
-template <int NR, class F>
-__device__ __forceinline__ void heavy_spmv(const int* __restrict__ ptr, int r, F f,
-                                           double* s0, double* s1, Smem& sm) {
-  const int p0 = ld_ro(ptr + r), p1 = ld_ro(ptr + r + 1);
-  double v[kNP];
-#pragma unroll
-  for (int s = 0; s < kNP; ++s) v[s] = 0.0;
-  for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) f(r, p, v[0], v[1]);
-  block_reduce(v, Ops{}, sm);
-  if (threadIdx.x == 0) {
-    s0[0] = sm.res[0];
-    if (NR == 2) s1[0] = sm.res[1];
-  }
-  __syncthreads();
-}
-
-// Row sums of a normal tile, CSR-stream style: every entry's product is
-// computed first (all loads and gathers of the tile independent of each
-// other), staged in shared memory, then each row is summed from there by L
-// lanes (each lane its strided entries in storage order, then a xor
-// butterfly; L == 1 is the sequential storage-order sum).  The order depends
-// only on the row and on L, never on the tile or the batch.
-// term(p, rhs) returns value[p] * x_rhs[index[p]].
-template <int NR, class F>
-__device__ __forceinline__ void stream_spmv(const Tile& t, int L, F term, Smem& sm) {
-  const int tid = threadIdx.x, BT = blockDim.x;
+  // tptr[0..rows] are the tile's row pointers (staged by the caller)
   const int rows = t.end - t.begin;
-  const int p0 = sm.ptr[0];
-  const int cnt = sm.ptr[rows] - p0;
+  const int p0 = tptr[0];
+  const int cnt = tptr[rows] - p0;
 #pragma unroll 1
   for (int rhs = 0; rhs < NR; ++rhs) {
-    for (int q0 = 0; q0 < cnt; q0 += 4 * BT) {
-      double v[4];
+    for (int q0 = 0; q0 < cnt; q0 += 8 * 32) {
+      double v[8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int q = q0 + u * BT + tid;
+      for (int u = 0; u < 8; ++u) {
+        const int q = q0 + u * 32 + lane;
         v[u] = q < cnt ? term(p0 + q, rhs) : 0.0;
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int q = q0 + u * BT + tid;
-        if (q < cnt) sm.prod[q] = v[u];
+      for (int u = 0; u < 8; ++u) {
+        const int q = q0 + u * 32 + lane;
+        if (q < cnt) W.sval[q] = v[u];
       }
     }
-    __syncthreads();
-    double* out = rhs == 0 ? sm.s0 : sm.s1;
-    const int lane = tid & (L - 1);
-    const int grp = tid / L, ngrp = BT / L;
+    __syncwarp();
+    double* out = rhs == 0 ? W.s0 : W.s1;
+    const int sub = lane & (L - 1);
+    const int grp = lane / L, ngrp = 32 / L;
     for (int rb = 0; rb < rows; rb += ngrp) {
       const int li = rb + grp;
       double a = 0.0;
       if (li < rows) {
-        const int e = sm.ptr[li + 1] - p0;
-        for (int q = sm.ptr[li] - p0 + lane; q < e; q += L) a += sm.prod[q];
+        const int e = tptr[li + 1] - p0;
+        int q = tptr[li] - p0 + sub;
+        for (; q + 7 * L < e; q += 8 * L) {
+          double v[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) v[u] = W.sval[q + u * L];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) a += v[u];
+        }
+        for (; q < e; q += L) a += W.sval[q];
       }
       for (int off = L >> 1; off > 0; off >>= 1) a += __shfl_xor_sync(kFull, a, off);
-      if (li < rows && lane == 0) out[li] = a;
+      if (li < rows && sub == 0) out[li] = a;
     }
-    __syncthreads();
+    __syncwarp();
   }
 }
 
-// Loads the tile's row pointers into shared memory (normal tiles).
-__device__ __forceinline__ void load_tile_ptr(const Tile& t, const int* ptr, Smem& sm) {
-  if (t.heavy) return;
-  const int rows = t.end - t.begin;
-  for (int i = threadIdx.x; i <= rows; i += blockDim.x) sm.ptr[i] = ld_ro(ptr + t.begin + i);
-  __syncthreads();
-}
-
-template <int NR, class F>
-__device__ __forceinline__ void tile_spmv(const Tile& t, const int* ptr, int L, F term, Smem& sm) {
-  if (t.heavy) {
-    auto f = [&](int r, int p, double& a0, double& a1) {
-      a0 += term(p, 0);
-      if (NR == 2) a1 += term(p, 1);
-    };
-    heavy_spmv<NR>(ptr, t.begin, f, sm.s0, sm.s1, sm);
-  } else {
-    load_tile_ptr(t, ptr, sm);
-    stream_spmv<NR>(t, L, term, sm);
-  }
-  __syncthreads();
-}
-
-// Max of |w| over each row after an optional in-place rescale (Ruiz pass).
-template <class F>
-__device__ __forceinline__ void tile_rowmax(const Tile& t, const int* ptr, int L, F f, Smem& sm) {
-  if (t.heavy) {
-    const int r = t.begin;
-    const int p0 = ld_ro(ptr + r), p1 = ld_ro(ptr + r + 1);
-    double v[kNP];
+// Row sums from staged products: prod[q] for the tile's entries, row li
+// spanning tptr[li]-p0 .. tptr[li+1]-p0; L lanes per row as in warp_spmv.
+__device__ __forceinline__ void staged_row_sums(const int* tptr, const double* prod, int rows,
+                                                int L, double* out, int lane) {
+  const int p0 = tptr[0];
+  const int sub = lane & (L - 1);
+  const int grp = lane / L, ngrp = 32 / L;
+  for (int rb = 0; rb < rows; rb += ngrp) {
+    const int li = rb + grp;
+    double a = 0.0;
+    if (li < rows) {
+      const int e = tptr[li + 1] - p0;
+      int q = tptr[li] - p0 + sub;
+      // eight loads in flight, the adds still in storage order
+      for (; q + 7 * L < e; q += 8 * L) {
+        double v[8];
 #pragma unroll
-    for (int s = 0; s < kNP; ++s) v[s] = 0.0;
-    for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) v[0] = fmax(v[0], f(r, p));
-    Ops o; o.maxmask = 1u;
-    block_reduce(v, o, sm);
-    if (threadIdx.x == 0) sm.s0[0] = sm.res[0];
+        for (int u = 0; u < 8; ++u) v[u] = prod[q + u * L];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) a += v[u];
+      }
+      for (; q < e; q += L) a += prod[q];
+    }
+    for (int off = L >> 1; off > 0; off >>= 1) a += __shfl_xor_sync(kFull, a, off);
+    if (li < rows && sub == 0) out[li] = a;
+  }
+  __syncwarp();
+}
+
+// Per-row max of f(r, p) over the tile (Ruiz pass); result in W.s0.
+template <class F>
+__device__ __forceinline__ void warp_rowmax(const Tile& t, const int* ptr, int L, F f,
+                                            WarpSmem& W, int lane) {
+  if (t.heavy) {
+    const int p0 = ld_ro(ptr + t.begin), p1 = ld_ro(ptr + t.begin + 1);
+    double a = 0.0;
+    for (int p = p0 + lane; p < p1; p += 32) a = fmax(a, f(t.begin, p));
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) a = fmax(a, __shfl_xor_sync(kFull, a, off));
+    if (lane == 0) W.s0[0] = a;
   } else {
-    const int tid = threadIdx.x;
-    const int lane = tid & (L - 1), grp = tid / L, ngrp = blockDim.x / L;
+    const int sub = lane & (L - 1), grp = lane / L, ngrp = 32 / L;
     for (int rb = t.begin; rb < t.end; rb += ngrp) {
       const int r = rb + grp;
       double a = 0.0;
       if (r < t.end) {
         const int p0 = ld_ro(ptr + r), p1 = ld_ro(ptr + r + 1);
-        for (int p = p0 + lane; p < p1; p += L) a = fmax(a, f(r, p));
+        for (int p = p0 + sub; p < p1; p += L) a = fmax(a, f(r, p));
       }
       for (int off = L >> 1; off > 0; off >>= 1) a = fmax(a, __shfl_xor_sync(kFull, a, off));
-      if (r < t.end && lane == 0) sm.s0[r - t.begin] = a;
+      if (r < t.end && sub == 0) W.s0[r - t.begin] = a;
     }
   }
-  __syncthreads();
+  __syncwarp();
 }
 
-// Elementwise pass over the entries of the tile's rows.
+// Elementwise pass over the entries of the tile's rows: f(r, p).
 template <class F>
-__device__ __forceinline__ void tile_entries(const Tile& t, const int* ptr, F f) {
-  if (t.heavy) {
-    const int r = t.begin;
+__device__ __forceinline__ void warp_entries(const Tile& t, const int* ptr, F f, int lane) {
+  for (int r = t.begin; r < t.end; ++r) {
     const int p0 = ld_ro(ptr + r), p1 = ld_ro(ptr + r + 1);
-    for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) f(r, p);
-  } else {
-    const int tid = threadIdx.x;
-    const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    for (int r = t.begin + warp; r < t.end; r += nw) {
-      const int p0 = ld_ro(ptr + r), p1 = ld_ro(ptr + r + 1);
-      for (int p = p0 + lane; p < p1; p += 32) f(r, p);
-    }
+    for (int p = p0 + lane; p < p1; p += 32) f(r, p);
   }
 }
 
-// Last row (exclusive) this thread visits in a thread-per-row loop over the
-// tile: all rows of a normal tile, only thread 0 for a heavy (single-row) tile.
-__device__ __forceinline__ int row_loop_end(const Tile& t) {
-  return t.heavy ? (threadIdx.x == 0 ? t.begin + 1 : t.begin) : t.end;
+// Last row (exclusive) this lane visits in a lane-per-row loop over the tile:
+// every row of a normal tile, only lane 0 for a heavy (single-row) tile.
+__device__ __forceinline__ int row_loop_end(const Tile& t, int lane) {
+  return t.heavy ? (lane == 0 ? t.begin + 1 : t.begin) : t.end;
 }
 
 // ---- small math shared by both sides -------------------------------------------

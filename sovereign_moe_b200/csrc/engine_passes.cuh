@@ -51,33 +51,76 @@ __device__ __forceinline__ double merit(double omega, double p, double d, double
 }
 
 // ---- finisher protocol ------------------------------------------------------
-
-// Called by every block after it wrote a tile's partials.  Returns true in the
-// block that completed the instance's last tile of this pass; that block then
-// sees every tile's partials.
-__device__ __forceinline__ bool finisher_enter(unsigned* cnt, int ntiles, Smem& sm) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();            // this block's tile partials (written by thread 0)
-    unsigned old = atomicAdd(cnt, 1u);
-    sm.flag = (old == (unsigned)(ntiles - 1));
+//
+// Two-level, fixed-order reduction of an instance's tile partials: the warp
+// that completes the last tile of a group (64 consecutive tiles of the
+// instance) sums the group's tile partials in tile order; the warp that
+// completes the instance's last group sums the group partials in group order
+// and advances the state machine.  Returns true in that warp, with the
+// instance's reduced values in res (every lane).
+__device__ __forceinline__ bool warp_finish(const EngineArgs& A, const Tile& t, int side,
+                                            int g_first, int g_last, bool need_red, Ops ops,
+                                            double* res, int lane) {
+  const int g = t.group;
+  const int2 gt = A.group_tiles[g];
+  const double* tp = A.partials + (side ? (size_t)A.n_rtiles * kNP : 0);
+  unsigned last = 0;
+  __syncwarp();
+  if (lane == 0)   // release this tile's partials; acquire the group's if last
+    last = atom_add_acq_rel(A.gcounters + g, 1u) == (unsigned)(gt.y - gt.x - 1);
+  last = __shfl_sync(kFull, last, 0);
+  if (!last) return false;
+  __syncwarp();                            // order the lanes' reads after lane 0's acquire
+  double v[kNP];
+  if (need_red) {
+#pragma unroll
+    for (int s = 0; s < kNP; ++s) v[s] = identity_of(ops.op(s));
+    for (int tt = gt.x + lane; tt < gt.y; tt += 32) {
+#pragma unroll
+      for (int s = 0; s < kNP; ++s) v[s] = combine(v[s], ld_mut(tp + (size_t)tt * kNP + s), ops.op(s));
+    }
+    warp_reduce(v, ops);
+    if (lane == 0) {
+#pragma unroll
+      for (int s = 0; s < kNP; ++s) A.gpartials[(size_t)g * kNP + s] = v[s];
+    }
   }
-  __syncthreads();
-  const bool last = sm.flag != 0;
-  if (last) __threadfence();
-  return last;
+  __syncwarp();
+  if (lane == 0) {
+    A.gcounters[g] = 0;
+    last = atom_add_acq_rel(A.counters + 2 * t.inst + side, 1u) == (unsigned)(g_last - g_first - 1);
+  }
+  last = __shfl_sync(kFull, last, 0);
+  if (!last) return false;
+  __syncwarp();
+  if (need_red) {
+#pragma unroll
+    for (int s = 0; s < kNP; ++s) v[s] = identity_of(ops.op(s));
+    for (int gg = g_first + lane; gg < g_last; gg += 32) {
+#pragma unroll
+      for (int s = 0; s < kNP; ++s) v[s] = combine(v[s], ld_mut(A.gpartials + (size_t)gg * kNP + s), ops.op(s));
+    }
+    warp_reduce(v, ops);
+#pragma unroll
+    for (int s = 0; s < kNP; ++s) res[s] = v[s];
+  }
+  if (lane == 0) A.counters[2 * t.inst + side] = 0;
+  return true;
 }
 
-// Reduce the instance's tile partials [tb, te) in a fixed order into sm.res.
-__device__ __forceinline__ void reduce_tiles(const double* partials, int tb, int te, Ops ops, Smem& sm) {
-  double v[kNP];
-#pragma unroll
-  for (int s = 0; s < kNP; ++s) v[s] = identity_of(ops.op(s));
-  for (int t = tb + threadIdx.x; t < te; t += blockDim.x) {
-#pragma unroll
-    for (int s = 0; s < kNP; ++s) v[s] = combine(v[s], ld_mut(partials + (size_t)t * kNP + s), ops.op(s));
+// Copy the tile's instance descriptor into the warp's shared memory (once per
+// run of tiles of the same instance).
+__device__ __forceinline__ const Inst& warp_inst(const EngineArgs& A, int inst, WarpSmem& W,
+                                                 int lane) {
+  if (W.inst_id != inst) {
+    const int* src = reinterpret_cast<const int*>(A.inst + inst);
+    int* dst = reinterpret_cast<int*>(&W.inst);
+    for (int i = lane; i < (int)(sizeof(Inst) / sizeof(int)); i += 32) dst[i] = src[i];
+    __syncwarp();
+    if (lane == 0) W.inst_id = inst;
+    __syncwarp();
   }
-  block_reduce(v, ops, sm);
+  return W.inst;
 }
 
 // ---- A pass ---------------------------------------------------------------
@@ -132,27 +175,235 @@ __device__ void r_finish(const EngineArgs& A, const Inst& I, State* S, int rmode
   }
 }
 
-// Copy the tile's instance descriptor into shared memory (once per run of
-// tiles of the same instance).
-__device__ __forceinline__ const Inst& cache_inst(const EngineArgs& A, int inst, Smem& sm) {
-  const bool need = sm.inst_id != inst;
-  __syncthreads();
-  if (need) {
-    const int* src = reinterpret_cast<const int*>(A.inst + inst);
-    int* dst = reinterpret_cast<int*>(&sm.inst);
-    for (int i = threadIdx.x; i < (int)(sizeof(Inst) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
-    __syncthreads();
-    if (threadIdx.x == 0) sm.inst_id = inst;
+__device__ void c_finish(const EngineArgs& A, const Inst& I, State* S, int cmode, const double* red);
+
+// ---- hot modes: staged tile passes ------------------------------------------
+//
+// The iteration (R_ITER, C_ITER), line-search trial (R_TRIAL) and primal step
+// (C_PRIMAL) passes run from shared memory: the tile's matrix arrays were
+// staged by the caller; here the epilogue vectors are staged while the gathers
+// are in flight, so a pass waits for about two global round trips.  The
+// arithmetic is exactly the generic passes' (same operands, same order).
+
+__device__ __forceinline__ void gather_products(const Tile& t, const double* src, WarpSmem& W,
+                                                int offi, int offv, int lane) {
+  double* prod = W.sval + offv;
+  const int* idx = W.sidx + offi;
+  const int cnt = t.cnt;
+  double g[kWTileNnz / 32];
+#pragma unroll
+  for (int u = 0; u < kWTileNnz / 32; ++u) {
+    const int q = lane + 32 * u;
+    g[u] = q < cnt ? ld_mut(src + idx[q]) : 0.0;
   }
-  return sm.inst;
+#pragma unroll
+  for (int u = 0; u < kWTileNnz / 32; ++u) {
+    const int q = lane + 32 * u;
+    if (q < cnt) prod[q] *= g[u];
+  }
+  __syncwarp();
 }
 
-__device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
-  const Tile t = A.rtiles[ti];
+__device__ void hot_rtile(const EngineArgs& A, const Tile& t, int ti, const Inst& I, State* S,
+                          WarpSmem& W, int lane, int rmode, bool commit, double eta,
+                          double omega, int offp, int offi, int offv) {
+#ifdef PDLP_TRACE
+  // stage timestamps of the first warp of block 0 (slots after the step trace)
+  // counter in trace[1279], records at trace[640 + 8 k], k < 63
+  long long* tq = (A.trace && blockIdx.x == 0 && threadIdx.x == 0) ? A.trace + 640 : nullptr;
+  long long tk = 0;
+  if (tq) { tk = A.trace[1279]; if (tk < 0 || tk >= 63) tq = nullptr; else tq += tk * 8; }
+#define HOT_STAMP(k) if (tq) tq[k] = global_ns()
+#else
+#define HOT_STAMP(k)
+#endif
+  HOT_STAMP(0);
+  const int rows = t.end - t.begin;
+  const double sigma = eta * omega;
+  // vectors: 0 ax, 1 y, 2 rl, 3 ru, 4 sum_y, 5 y_new, 6 adx
+  const int off = stage<8>(W.vec[0], I.ax, t.begin, rows, lane);
+  stage<8>(W.vec[1], I.y, t.begin, rows, lane);
+  stage<8>(W.vec[2], I.rl, t.begin, rows, lane);
+  stage<8>(W.vec[3], I.ru, t.begin, rows, lane);
+  if (rmode == R_ITER || commit) stage<8>(W.vec[4], I.sumy, t.begin, rows, lane);
+  if (commit) {
+    stage<8>(W.vec[5], I.ynew, t.begin, rows, lane);
+    stage<8>(W.vec[6], I.adx, t.begin, rows, lane);
+  }
+  cp_async_commit();
+  HOT_STAMP(1);
+  cp_async_wait<1>();
+  __syncwarp();
+  HOT_STAMP(2);
+  gather_products(t, I.dx, W, offi, offv, lane);
+  HOT_STAMP(3);
+  staged_row_sums(W.sptr + offp, W.sval + offv, rows, I.lanes_r, W.s0, lane);
+  HOT_STAMP(4);
+  cp_async_wait<0>();
+  __syncwarp();
+  HOT_STAMP(5);
+  double acc[kNP];
+#pragma unroll
+  for (int s = 0; s < kNP; ++s) acc[s] = 0.0;
+  for (int li = lane; li < rows; li += 32) {
+    const int r = t.begin + li;
+    const int v = off + li;
+    double ax = W.vec[0][v], y = W.vec[1][v], sumy = W.vec[4][v];
+    const double rl = W.vec[2][v], ru = W.vec[3][v];
+    if (commit) {                     // pdlp.py:385-389
+      const double yn = W.vec[5][v];
+      y = yn;
+      ax = ax + W.vec[6][v];
+      sumy = sumy + eta * yn;
+      I.y[r] = y;
+      I.ax[r] = ax;
+      I.sumy[r] = sumy;
+    }
+    const double a = W.s0[li];
+    if (rmode == R_ITER) {            // backend.py:260-279
+      const double axn = ax + a;
+      I.ax[r] = axn;
+      const double w = y + sigma * (axn + a);
+      const double yn = prox(w, sigma, rl, ru);
+      I.dy[r] = yn - y;
+      I.y[r] = yn;
+      I.sumy[r] = sumy + eta * yn;
+    } else {                          // pdlp.py:347-356
+      I.adx[r] = a;
+      const double axb = ax + 2.0 * a;
+      const double w = y + sigma * axb;
+      const double yn = prox(w, sigma, rl, ru);
+      I.ynew[r] = yn;
+      const double d = yn - y;
+      I.dy[r] = d;
+      acc[0] += d * a;
+      acc[1] += d * d;
+    }
+  }
+  HOT_STAMP(6);
+#ifdef PDLP_TRACE
+  if (tq) A.trace[1279] = tk + 1;
+#endif
+#undef HOT_STAMP
+  const bool need_red = rmode == R_TRIAL;
+  const bool need_fin = need_red || commit;
+  Ops ops;
+  if (need_red) {
+    warp_reduce(acc, ops);
+    if (lane == 0) {
+#pragma unroll
+      for (int s = 0; s < kNP; ++s) A.partials[(size_t)ti * kNP + s] = acc[s];
+    }
+  }
+  if (!need_fin) return;
+  double res[kNP];
+  if (warp_finish(A, t, 0, I.rg_begin, I.rg_end, need_red, ops, res, lane)) {
+    if (lane == 0) r_finish(A, I, S, rmode, res);
+    __syncwarp();
+  }
+}
+
+__device__ void hot_ctile(const EngineArgs& A, const Tile& t, int ti, const Inst& I, State* S,
+                          WarpSmem& W, int lane, int cmode, int cprimal, bool xcommit,
+                          double eta, double omega, int offp, int offi, int offv) {
+  const int rows = t.end - t.begin;
+  const double tau = eta / omega;
+  const bool iter = cmode == C_ITER;
+  const bool xc = iter && xcommit;
+  // vectors: 0 aty, 1 x (x_new on a commit), 2 c, 3 lo, 4 hi, 5 sum_x
+  const int off = stage<8>(W.vec[0], I.aty, t.begin, rows, lane);
+  stage<8>(W.vec[1], xc ? I.xnew : I.x, t.begin, rows, lane);
+  stage<8>(W.vec[2], I.c, t.begin, rows, lane);
+  stage<8>(W.vec[3], I.lo, t.begin, rows, lane);
+  stage<8>(W.vec[4], I.hi, t.begin, rows, lane);
+  if (iter) stage<8>(W.vec[5], I.sumx, t.begin, rows, lane);
+  cp_async_commit();
+  if (iter) {
+    cp_async_wait<1>();
+    __syncwarp();
+    gather_products(t, I.dy, W, offi, offv, lane);
+    staged_row_sums(W.sptr + offp, W.sval + offv, rows, I.lanes_c, W.s0, lane);
+  }
+  cp_async_wait<0>();
+  __syncwarp();
+  double acc[kNP];
+#pragma unroll
+  for (int s = 0; s < kNP; ++s) acc[s] = 0.0;
+  for (int li = lane; li < rows; li += 32) {
+    const int j = t.begin + li;
+    const int v = off + li;
+    const double xv = W.vec[1][v];
+    double atyv = W.vec[0][v];
+    if (iter) {                       // backend.py:282-291
+      atyv = atyv + W.s0[li];
+      I.aty[j] = atyv;
+      I.sumx[j] = W.vec[5][v] + eta * xv;
+    }
+    if (cprimal == P_NONE) {
+      if (xc) I.x[j] = xv;
+    } else {                          // backend.py:204-215 / 241-255
+      const double xn = clip(xv - tau * (W.vec[2][v] + atyv), W.vec[3][v], W.vec[4][v]);
+      const double d = xn - xv;
+      I.dx[j] = d;
+      if (cprimal == P_TRIAL) {
+        I.xnew[j] = xn;
+        if (xc) I.x[j] = xv;
+        acc[0] += d * d;
+      } else {
+        I.x[j] = xn;
+      }
+    }
+  }
+  const bool need_red = cprimal == P_TRIAL;
+  Ops ops;
+  if (need_red) {
+    warp_reduce(acc, ops);
+    if (lane == 0) {
+#pragma unroll
+      for (int s = 0; s < kNP; ++s) A.partials[(size_t)(A.n_rtiles + ti) * kNP + s] = acc[s];
+    }
+  }
+  double res[kNP];
+  if (warp_finish(A, t, 1, I.cg_begin, I.cg_end, need_red, ops, res, lane)) {
+    if (lane == 0) c_finish(A, I, S, cmode, res);
+    __syncwarp();
+  }
+}
+
+__device__ void process_rtile(const EngineArgs& A, const Tile t, int ti, WarpSmem& W, int lane) {
+#ifdef PDLP_TRACE
+  if (A.trace && blockIdx.x == 0 && threadIdx.x == 0) {
+    const long long k = A.trace[1279];
+    if (k >= 0 && k < 63) A.trace[640 + k * 8 + 7] = global_ns();
+  }
+#endif
   State* S = A.st + t.inst;
+  const Inst& I = warp_inst(A, t.inst, W, lane);
+  // The tile's row pointers, indices and values are immutable: their copies
+  // to shared memory start before the state is read, so the state load and
+  // the matrix stream overlap.
+  int offp = 0, offi = 0, offv = 0;
+  if (!t.heavy) {
+    offp = stage<4>(W.sptr, I.rp, t.begin, t.end - t.begin + 1, lane);
+    offi = stage<4>(W.sidx, I.ri, t.p0, t.cnt, lane);
+    offv = stage<8>(W.sval, I.rx, t.p0, t.cnt, lane);
+  }
+  cp_async_commit();
   const int rmode = ld_mut(&S->rmode);
-  if (rmode == R_NONE) return;
-  const Inst& I = cache_inst(A, t.inst, sm);
+  const bool commit = ld_mut(&S->ycommit) != 0;
+  const double eta = ld_mut(&S->eta), omega = ld_mut(&S->omega);
+  if (rmode == R_NONE) {
+    cp_async_wait<0>();
+    __syncwarp();
+    return;
+  }
+  if ((rmode == R_ITER || rmode == R_TRIAL) && !t.heavy) {
+    hot_rtile(A, t, ti, I, S, W, lane, rmode, commit, eta, omega, offp, offi, offv);
+    return;
+  }
+  cp_async_wait<0>();
+  __syncwarp();
+  const int* tptr = W.sptr + offp;
 
   const int L = I.lanes_r;
   const int* __restrict__ rp = I.rp;
@@ -161,9 +412,7 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
 #pragma unroll
   for (int s = 0; s < kNP; ++s) acc[s] = 0.0;
   Ops ops;
-  const int rend = row_loop_end(t);
-  const bool commit = ld_mut(&S->ycommit) != 0;
-  const double eta = ld_mut(&S->eta), omega = ld_mut(&S->omega);
+  const int rend = row_loop_end(t, lane);
   const double sigma = eta * omega;
 
   // pending commit of an accepted line-search trial (pdlp.py:385-389):
@@ -186,20 +435,20 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
       const double* dc_old = (it - 1) & 1 ? I.xnew : I.dx;
       double* dr_new = it & 1 ? I.ynew : I.dy;
       double* rr = I.yrst;                                      // running Ruiz row factor
-      tile_rowmax(t, rp, L, [&](int r, int p) {
+      warp_rowmax(t, rp, L, [&](int r, int p) {
         double v = it <= 1 ? ld_ro(src + p) : ld_mut(src + p);
         if (it >= 1) {
           v = v * (ld_mut(dr_old + r) * ld_mut(dc_old + ld_ro(ri + p)));
           I.rx[p] = v;
         }
         return fabs(v);
-      }, sm);
+      }, W, lane);
       ops.maxmask = 1u;
-      for (int r = t.begin + threadIdx.x; r < rend; r += blockDim.x) {
+      for (int r = t.begin + lane; r < rend; r += 32) {
         const int li = r - t.begin;
         rr[r] = it == 0 ? 1.0 : ld_mut(rr + r) * ld_mut(dr_old + r);
         if (!last) {
-          double rmax = sm.s0[li];
+          double rmax = W.s0[li];
           if (rmax <= 0.0) rmax = 1.0;
           acc[0] = fmax(acc[0], fabs(1.0 - rmax));
           dr_new[r] = 1.0 / sqrt(rmax);
@@ -213,7 +462,7 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
       const double* rr = I.yrst;
       const double* cr = I.xrst;
       const bool have_ruiz = I.ruiz_iters > 0;
-      for (int r = t.begin + threadIdx.x; r < rend; r += blockDim.x) {
+      for (int r = t.begin + lane; r < rend; r += 32) {
         const double ri_r = have_ruiz ? ld_mut(rr + r) : 1.0;
         double f;
         if (I.scale_none) {
@@ -235,11 +484,11 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
       break;
     }
     case R_APPLY: {
-      tile_entries(t, rp, [&](int r, int p) {
+      warp_entries(t, rp, [&](int r, int p) {
         I.rx[p] = ld_ro(I.rx0 + p) * (ld_mut(I.rs + r) * ld_mut(I.cs + ld_ro(ri + p)));
-      });
+      }, lane);
       ops.maxmask = 1u;
-      for (int r = t.begin + threadIdx.x; r < rend; r += blockDim.x) {
+      for (int r = t.begin + lane; r < rend; r += 32) {
         const double s = ld_mut(I.rs + r);
         const double l0 = ld_ro(I.rl0 + r), u0 = ld_ro(I.ru0 + r);
         const double l = row_bound(l0, s), u = row_bound(u0, s);
@@ -252,7 +501,7 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
       break;
     }
     case R_SETUP0: {
-      for (int r = t.begin + threadIdx.x; r < rend; r += blockDim.x) {
+      for (int r = t.begin + lane; r < rend; r += 32) {
         I.y[r] = 0.0; I.sumy[r] = 0.0; I.yrst[r] = 0.0; I.dy[r] = 0.0;
       }
       break;
@@ -268,14 +517,14 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
         if (rhs == 0) return a * (scale != 0.0 ? ld_mut(v + j) / scale : 0.0);
         return a * ld_mut(I.x + j);
       };
-      if (round == 1) tile_spmv<2>(t, rp, L, term, sm);
-      else tile_spmv<1>(t, rp, L, term, sm);
+      if (round == 1) warp_spmv<2>(t, rp, tptr, L, term, W, lane);
+      else warp_spmv<1>(t, rp, tptr, L, term, W, lane);
       ops.maxmask = 1u;
-      for (int r = t.begin + threadIdx.x; r < rend; r += blockDim.x) {
+      for (int r = t.begin + lane; r < rend; r += 32) {
         const int li = r - t.begin;
-        I.ybar[r] = sm.s0[li];
+        I.ybar[r] = W.s0[li];
         if (round == 1) {
-          const double axv = sm.s1[li];
+          const double axv = W.s1[li];
           I.ax[r] = axv;
           acc[0] = fmax(acc[0], pviol(axv, ld_mut(I.rl + r), ld_mut(I.ru + r)));
         }
@@ -286,12 +535,12 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
       // backend.py:260-279: ax += adx; w = y + sigma (ax + adx); prox; dy
       const double* rx = I.rx;
       const double* dxv = I.dx;
-      tile_spmv<1>(t, rp, L, [&](int p, int) {
+      warp_spmv<1>(t, rp, tptr, L, [&](int p, int) {
         return ld_mut(rx + p) * ld_mut(dxv + ld_ro(ri + p));
-      }, sm);
-      for (int r = t.begin + threadIdx.x; r < rend; r += blockDim.x) {
+      }, W, lane);
+      for (int r = t.begin + lane; r < rend; r += 32) {
         do_commit(r);
-        const double a = sm.s0[r - t.begin];
+        const double a = W.s0[r - t.begin];
         const double axn = ld_mut(I.ax + r) + a;
         I.ax[r] = axn;
         const double yo = ld_mut(I.y + r);
@@ -307,12 +556,12 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
       // pdlp.py:347-356: adx = A dx; ax_bar = ax + 2 adx; dual_step; dy; dots
       const double* rx = I.rx;
       const double* dxv = I.dx;
-      tile_spmv<1>(t, rp, L, [&](int p, int) {
+      warp_spmv<1>(t, rp, tptr, L, [&](int p, int) {
         return ld_mut(rx + p) * ld_mut(dxv + ld_ro(ri + p));
-      }, sm);
-      for (int r = t.begin + threadIdx.x; r < rend; r += blockDim.x) {
+      }, W, lane);
+      for (int r = t.begin + lane; r < rend; r += 32) {
         do_commit(r);
-        const double a = sm.s0[r - t.begin];
+        const double a = W.s0[r - t.begin];
         I.adx[r] = a;
         const double axb = ld_mut(I.ax + r) + 2.0 * a;
         const double yo = ld_mut(I.y + r);
@@ -329,7 +578,7 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
     case R_CHECK_A: {
       const double se = ld_mut(&S->sum_eta);
       ops.maxmask = 1u;
-      for (int r = t.begin + threadIdx.x; r < rend; r += blockDim.x) {
+      for (int r = t.begin + lane; r < rend; r += 32) {
         do_commit(r);
         const double yv = ld_mut(I.y + r);
         const double yb = se > 0.0 ? ld_mut(I.sumy + r) / se : yv;
@@ -348,14 +597,14 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
       const double* rx = I.rx;
       const double* xb = I.xbar;
       const double* xc = I.x;
-      tile_spmv<2>(t, rp, L, [&](int p, int rhs) {
+      warp_spmv<2>(t, rp, tptr, L, [&](int p, int rhs) {
         const int j = ld_ro(ri + p);
         return ld_mut(rx + p) * ld_mut((rhs == 0 ? xb : xc) + j);
-      }, sm);
+      }, W, lane);
       ops.maxmask = 7u;
-      for (int r = t.begin + threadIdx.x; r < rend; r += blockDim.x) {
+      for (int r = t.begin + lane; r < rend; r += 32) {
         const int li = r - t.begin;
-        const double axb = sm.s0[li], axf = sm.s1[li];
+        const double axb = W.s0[li], axf = W.s1[li];
         I.axbar[r] = axb;
         I.axf[r] = axf;
         const double l = ld_mut(I.rl + r), u = ld_mut(I.ru + r), s = ld_mut(I.rs + r);
@@ -368,7 +617,7 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
     }
     case R_RESTART: {
       const bool avg = ld_mut(&S->restart_src) != 0;
-      for (int r = t.begin + threadIdx.x; r < rend; r += blockDim.x) {
+      for (int r = t.begin + lane; r < rend; r += 32) {
         double yv;
         if (avg) { yv = ld_mut(I.ybar + r); I.y[r] = yv; I.ax[r] = ld_mut(I.axbar + r); }
         else { yv = ld_mut(I.y + r); I.ax[r] = ld_mut(I.axf + r); }
@@ -381,7 +630,7 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
       const bool avg = ld_mut(&S->final_src) != 0;
       const double s = ld_mut(&S->s_obj);
       const double ysign = I.sense == 1 ? -1.0 : 1.0;
-      for (int r = t.begin + threadIdx.x; r < rend; r += blockDim.x) {
+      for (int r = t.begin + lane; r < rend; r += 32) {
         do_commit(r);
         const double yv = avg ? ld_mut(I.ybar + r) : ld_mut(I.y + r);
         I.yout[r] = ysign * ((yv * ld_mut(I.rs + r)) / s);
@@ -397,23 +646,17 @@ __device__ void process_rtile(const EngineArgs& A, int ti, Smem& sm) {
                         rmode == R_TRIAL || rmode == R_CHECK_A || rmode == R_CHECK_B;
   const bool need_fin = !(rmode == R_ITER && !commit);
   if (need_red) {
-    block_reduce(acc, ops, sm);
-    if (threadIdx.x == 0) {
+    warp_reduce(acc, ops);
+    if (lane == 0) {
 #pragma unroll
-      for (int s = 0; s < kNP; ++s) A.partials[(size_t)ti * kNP + s] = sm.res[s];
+      for (int s = 0; s < kNP; ++s) A.partials[(size_t)ti * kNP + s] = acc[s];
     }
   }
   if (!need_fin) return;
-  const int ntiles = I.rt_end - I.rt_begin;
-  const int rt0 = I.rt_begin, rt1 = I.rt_end;
-  if (finisher_enter(A.counters + 2 * t.inst, ntiles, sm)) {
-    if (need_red) reduce_tiles(A.partials, rt0, rt1, ops, sm);
-    if (threadIdx.x == 0) {
-      r_finish(A, I, S, rmode, sm.res);
-      A.counters[2 * t.inst] = 0;
-      __threadfence();
-    }
-    __syncthreads();
+  double res[kNP];
+  if (warp_finish(A, t, 0, I.rg_begin, I.rg_end, need_red, ops, res, lane)) {
+    if (lane == 0) r_finish(A, I, S, rmode, res);
+    __syncwarp();
   }
 }
 
@@ -614,13 +857,32 @@ __device__ void c_finish(const EngineArgs& A, const Inst& I, State* S, int cmode
   }
 }
 
-__device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
-  const Tile t = A.ctiles[ti];
+__device__ void process_ctile(const EngineArgs& A, const Tile t, int ti, WarpSmem& W, int lane) {
   State* S = A.st + t.inst;
+  const Inst& I = warp_inst(A, t.inst, W, lane);
+  int offp = 0, offi = 0, offv = 0;
+  if (!t.heavy) {
+    offp = stage<4>(W.sptr, I.cp, t.begin, t.end - t.begin + 1, lane);
+    offi = stage<4>(W.sidx, I.ci, t.p0, t.cnt, lane);
+    offv = stage<8>(W.sval, I.cx, t.p0, t.cnt, lane);
+  }
+  cp_async_commit();
   const int cmode = ld_mut(&S->cmode);
-  if (cmode == C_NONE) return;
-  const Inst& I = cache_inst(A, t.inst, sm);
   const int cprimal = ld_mut(&S->cprimal);
+  const bool xcommit = ld_mut(&S->xcommit) != 0;
+  const double eta = ld_mut(&S->eta), omega = ld_mut(&S->omega);
+  if (cmode == C_NONE) {
+    cp_async_wait<0>();
+    __syncwarp();
+    return;
+  }
+  if ((cmode == C_ITER || cmode == C_PRIMAL) && !t.heavy) {
+    hot_ctile(A, t, ti, I, S, W, lane, cmode, cprimal, xcommit, eta, omega, offp, offi, offv);
+    return;
+  }
+  cp_async_wait<0>();
+  __syncwarp();
+  const int* tptr = W.sptr + offp;
 
   const int L = I.lanes_c;
   const int* __restrict__ cp = I.cp;
@@ -629,8 +891,7 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
 #pragma unroll
   for (int s = 0; s < kNP; ++s) acc[s] = 0.0;
   Ops ops;
-  const int rend = row_loop_end(t);
-  const double eta = ld_mut(&S->eta), omega = ld_mut(&S->omega);
+  const int rend = row_loop_end(t, lane);
   const double tau = eta / omega;
 
   switch (cmode) {
@@ -642,20 +903,20 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
       const double* dc_old = (it - 1) & 1 ? I.xnew : I.dx;
       double* dc_new = it & 1 ? I.xnew : I.dx;
       double* cr = I.xrst;
-      tile_rowmax(t, cp, L, [&](int j, int p) {
+      warp_rowmax(t, cp, L, [&](int j, int p) {
         double v = it <= 1 ? ld_ro(src + p) : ld_mut(src + p);
         if (it >= 1) {
           v = v * (ld_mut(dr_old + ld_ro(ci + p)) * ld_mut(dc_old + j));
           I.cx[p] = v;
         }
         return fabs(v);
-      }, sm);
+      }, W, lane);
       ops.maxmask = 1u;
-      for (int j = t.begin + threadIdx.x; j < rend; j += blockDim.x) {
+      for (int j = t.begin + lane; j < rend; j += 32) {
         const int li = j - t.begin;
         cr[j] = it == 0 ? 1.0 : ld_mut(cr + j) * ld_mut(dc_old + j);
         if (!last) {
-          double cmax = sm.s0[li];
+          double cmax = W.s0[li];
           if (cmax <= 0.0) cmax = 1.0;
           acc[0] = fmax(acc[0], fabs(1.0 - cmax));
           dc_new[j] = 1.0 / sqrt(cmax);
@@ -667,7 +928,7 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
       const double* rr = I.yrst;
       const double* cr = I.xrst;
       const bool have_ruiz = I.ruiz_iters > 0;
-      for (int j = t.begin + threadIdx.x; j < rend; j += blockDim.x) {
+      for (int j = t.begin + lane; j < rend; j += 32) {
         const double cj = have_ruiz ? ld_mut(cr + j) : 1.0;
         double f;
         if (I.scale_none) {
@@ -690,13 +951,13 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
       break;
     }
     case C_APPLY: {
-      tile_entries(t, cp, [&](int j, int p) {
+      warp_entries(t, cp, [&](int j, int p) {
         I.cx[p] = ld_ro(I.cx0 + p) * (ld_mut(I.rs + ld_ro(ci + p)) * ld_mut(I.cs + j));
-      });
+      }, lane);
       ops.maxmask = 5u;       // slots 0 and 2
       ops.minmask = 2u;       // slot 1
       acc[1] = INFINITY;
-      for (int j = t.begin + threadIdx.x; j < rend; j += blockDim.x) {
+      for (int j = t.begin + lane; j < rend; j += 32) {
         const double s = ld_mut(I.cs + j);
         const double c0 = ld_ro(I.c0 + j);
         const double cw = I.sense == 1 ? c0 : -c0;
@@ -715,7 +976,7 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
     case C_SETUP0: {
       const double s = ld_mut(&S->s_obj);
       ops.maxmask = 4u;       // slot 2
-      for (int j = t.begin + threadIdx.x; j < rend; j += blockDim.x) {
+      for (int j = t.begin + lane; j < rend; j += 32) {
         const double c = ld_mut(I.c + j) * s;
         I.c[j] = c;
         const double l = ld_mut(I.lo + j), h = ld_mut(I.hi + j);
@@ -735,11 +996,11 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
     case C_POWER: {
       const double* cx = I.cx;
       const double* av = I.ybar;
-      tile_spmv<1>(t, cp, L, [&](int p, int) {
+      warp_spmv<1>(t, cp, tptr, L, [&](int p, int) {
         return ld_mut(cx + p) * ld_mut(av + ld_ro(ci + p));
-      }, sm);
-      for (int j = t.begin + threadIdx.x; j < rend; j += blockDim.x) {
-        const double v = sm.s0[j - t.begin];
+      }, W, lane);
+      for (int j = t.begin + lane; j < rend; j += 32) {
+        const double v = W.s0[j - t.begin];
         I.xbar[j] = v;
         acc[0] += v * v;
       }
@@ -748,15 +1009,15 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
     case C_ITER: {
       // backend.py:282-291 (aty += ady; sum_x += eta x) then the next primal step
       const double* cx = I.cx;
-      const bool xc = ld_mut(&S->xcommit) != 0;
+      const bool xc = xcommit;
       const int kind = cprimal;
       const double* dyv = I.dy;
-      tile_spmv<1>(t, cp, L, [&](int p, int) {
+      warp_spmv<1>(t, cp, tptr, L, [&](int p, int) {
         return ld_mut(cx + p) * ld_mut(dyv + ld_ro(ci + p));
-      }, sm);
-      for (int j = t.begin + threadIdx.x; j < rend; j += blockDim.x) {
+      }, W, lane);
+      for (int j = t.begin + lane; j < rend; j += 32) {
         const double xv = xc ? ld_mut(I.xnew + j) : ld_mut(I.x + j);
-        const double atyv = ld_mut(I.aty + j) + sm.s0[j - t.begin];
+        const double atyv = ld_mut(I.aty + j) + W.s0[j - t.begin];
         I.aty[j] = atyv;
         I.sumx[j] = ld_mut(I.sumx + j) + eta * xv;
         if (kind == P_NONE) {
@@ -769,14 +1030,14 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
     }
     case C_PRIMAL: {
       const int kind = cprimal;
-      for (int j = t.begin + threadIdx.x; j < rend; j += blockDim.x)
+      for (int j = t.begin + lane; j < rend; j += 32)
         acc[0] += primal_half(I, j, ld_mut(I.x + j), ld_mut(I.aty + j), tau, kind, false);
       break;
     }
     case C_CHECK_A: {
       const double se = ld_mut(&S->sum_eta);
       ops.maxmask = 1u;
-      for (int j = t.begin + threadIdx.x; j < rend; j += blockDim.x) {
+      for (int j = t.begin + lane; j < rend; j += 32) {
         const double xv = ld_mut(I.x + j);
         const double xb = se > 0.0 ? ld_mut(I.sumx + j) / se : xv;
         I.xbar[j] = xb;
@@ -796,15 +1057,15 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
       const double* cx = I.cx;
       const double* yb = I.ybar;
       const double* yc = I.y;
-      tile_spmv<2>(t, cp, L, [&](int p, int rhs) {
+      warp_spmv<2>(t, cp, tptr, L, [&](int p, int rhs) {
         const int i = ld_ro(ci + p);
         return ld_mut(cx + p) * ld_mut((rhs == 0 ? yb : yc) + i);
-      }, sm);
+      }, W, lane);
       const double s = ld_mut(&S->s_obj);
       ops.maxmask = (1u << 0) | (1u << 2) | (1u << 3) | (1u << 4) | (1u << 6);
-      for (int j = t.begin + threadIdx.x; j < rend; j += blockDim.x) {
+      for (int j = t.begin + lane; j < rend; j += 32) {
         const int li = j - t.begin;
-        const double atb = sm.s0[li], atf = sm.s1[li];
+        const double atb = W.s0[li], atf = W.s1[li];
         I.atybar[j] = atb;
         I.atyf[j] = atf;
         const double c = ld_mut(I.c + j), l = ld_mut(I.lo + j), h = ld_mut(I.hi + j);
@@ -824,7 +1085,7 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
     case C_RESTART: {
       const bool avg = ld_mut(&S->restart_src) != 0;
       const int kind = cprimal;
-      for (int j = t.begin + threadIdx.x; j < rend; j += blockDim.x) {
+      for (int j = t.begin + lane; j < rend; j += 32) {
         const double xv = avg ? ld_mut(I.xbar + j) : ld_mut(I.x + j);
         const double atyv = avg ? ld_mut(I.atybar + j) : ld_mut(I.atyf + j);
         I.x[j] = xv;
@@ -841,17 +1102,17 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
       const bool avg = ld_mut(&S->final_src) != 0;
       const double* ysrc = avg ? I.ybar : I.y;
       const double* cx = I.cx;
-      tile_spmv<1>(t, cp, L, [&](int p, int) {
+      warp_spmv<1>(t, cp, tptr, L, [&](int p, int) {
         return ld_mut(cx + p) * ld_mut(ysrc + ld_ro(ci + p));
-      }, sm);
+      }, W, lane);
       const double s = ld_mut(&S->s_obj);
       const double dsign = I.sense == 1 ? 1.0 : -1.0;
-      for (int j = t.begin + threadIdx.x; j < rend; j += blockDim.x) {
+      for (int j = t.begin + lane; j < rend; j += 32) {
         const double cs = ld_mut(I.cs + j);
         const double xv = avg ? ld_mut(I.xbar + j) : ld_mut(I.x + j);
         const double xo = clip(xv * cs, ld_ro(I.lo0 + j), ld_ro(I.hi0 + j));
         I.xout[j] = xo;
-        I.dout[j] = dsign * ((ld_mut(I.c + j) + sm.s0[j - t.begin]) / (s * cs));
+        I.dout[j] = dsign * ((ld_mut(I.c + j) + W.s0[j - t.begin]) / (s * cs));
         acc[0] += ld_ro(I.c0 + j) * xo;
       }
       break;
@@ -865,23 +1126,17 @@ __device__ void process_ctile(const EngineArgs& A, int ti, Smem& sm) {
                         cmode == C_POWER || cmode == C_CHECK_A || cmode == C_CHECK_B ||
                         cmode == C_FINAL;
   if (need_red) {
-    block_reduce(acc, ops, sm);
-    if (threadIdx.x == 0) {
+    warp_reduce(acc, ops);
+    if (lane == 0) {
 #pragma unroll
       for (int s = 0; s < kNP; ++s)
-        A.partials[(size_t)(A.n_rtiles + ti) * kNP + s] = sm.res[s];
+        A.partials[(size_t)(A.n_rtiles + ti) * kNP + s] = acc[s];
     }
   }
-  const int ntiles = I.ct_end - I.ct_begin;
-  const int ct0 = I.ct_begin, ct1 = I.ct_end;
-  if (finisher_enter(A.counters + 2 * t.inst + 1, ntiles, sm)) {
-    if (need_red) reduce_tiles(A.partials + (size_t)A.n_rtiles * kNP, ct0, ct1, ops, sm);
-    if (threadIdx.x == 0) {
-      c_finish(A, I, S, cmode, sm.res);
-      A.counters[2 * t.inst + 1] = 0;
-      __threadfence();
-    }
-    __syncthreads();
+  double res[kNP];
+  if (warp_finish(A, t, 1, I.cg_begin, I.cg_end, need_red, ops, res, lane)) {
+    if (lane == 0) c_finish(A, I, S, cmode, res);
+    __syncwarp();
   }
 }
 

@@ -363,7 +363,9 @@ def run_gpu(args, rank, world):
     value = N_LP * world / (step_ms / 1000.0)
     eng_ms, eng_bytes, eng_launches = arm.engine_ms, arm.engine_bytes, arm.engine_launches
 
-    # end to end through the C ABI from pinned host buffers
+    # end to end through the C ABI from pinned host buffers (one untimed pass
+    # first, so both arms are timed warm)
+    arm.step(host=True)
     barrier()
     ev0.record()
     for _ in range(args.steps):
@@ -416,6 +418,95 @@ def run_gpu(args, rank, world):
     return 0
 
 
+# --------------------------------------------------------------------------- #
+# auxiliary workloads (one JSON line each; not the headline metric)            #
+# --------------------------------------------------------------------------- #
+
+def _sync_events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def run_blend(args):
+    """Single large LP (200k x 600k, 3M nnz, 720-period blending plan,
+    log-uniform values): float64 vs float32-SpMV iteration throughput and the
+    engine kernel's achieved bandwidth over a fixed number of iterations."""
+    import torch
+    from sovereign_moe_b200.batch import BatchEngine
+    from sovereign_moe_b200.pdlp import PDLPParams
+    from sovereign_moe_b200.workloads import blending_plan
+    k = blending_plan(seed=0)
+    peak, kind = load_peaks()
+    out = {"workload": "blending_plan_200k_x_600k", "nnz": int(k.problem.nnz),
+           "iterations": args.iters}
+    for prec in ("fp64", "fp32"):
+        p = PDLPParams(device="gpu", eps_abs=1e-6, eps_rel=1e-6, max_iter=args.iters,
+                       precision=prec)
+        with BatchEngine(max_slots=1) as eng:
+            slot = eng.admit(k.problem, p)
+            ms = by = 0.0
+            its = 0
+            while True:
+                a = eng.step(256)
+                m_, b_, i_ = eng.last_timing()
+                ms += m_
+                by += b_
+                its += i_
+                if a == 0:
+                    break
+            r = eng.poll(slot)
+            out[prec] = {"ms": ms, "iters": int(r.iterations), "status": int(r.status),
+                         "us_per_iter": 1000.0 * ms / max(1, r.iterations),
+                         "achieved_GBps": by / ms / 1e6 if ms else 0.0,
+                         "frac_of_measured_hbm": by / ms / 1e6 / peak if ms else 0.0}
+    print(json.dumps({"metric": "PDHG iteration bandwidth (single LP)", "config": out,
+                      "peak_GBps": peak, "peak_source": kind}), flush=True)
+    return 0
+
+
+def run_powerlaw(args):
+    """1M x 3M, 10M nnz power-law LP: float32 PDHG inner solves, float64
+    refinement to rel KKT 1e-8; error against the known optimum."""
+    from sovereign_moe_b200.pdlp import PDLPParams
+    from sovereign_moe_b200.refine import solve_refined
+    from sovereign_moe_b200.workloads import power_law
+    scale = args.scale
+    k = power_law(seed=0, m=int(1_000_000 * scale), n=int(3_000_000 * scale),
+                  nnz=int(10_000_000 * scale))
+    t = time.perf_counter()
+    s = solve_refined(k.problem, PDLPParams(device="gpu", max_iter=args.iters,
+                                            time_limit=args.time_limit), target=1e-8)
+    dt = time.perf_counter() - t
+    rel = abs(s.objective - k.f_star) / max(1.0, abs(k.f_star))
+    print(json.dumps({"metric": "time to rel KKT 1e-8 (refined)", "value": dt, "unit": "s",
+                      "status": int(s.status), "rel_obj_err_vs_known": rel,
+                      "inner_iterations": int(s.iterations), "rounds": s.log,
+                      "config": {"workload": f"power_law_{k.problem.m}x{k.problem.n}",
+                                 "nnz": int(k.problem.nnz)}}), flush=True)
+    return 0
+
+
+def run_serving(args):
+    """Poisson arrivals served with continuous batching vs one at a time."""
+    from sovereign_moe_b200.serving import Server, latency_summary, serve_one_at_a_time
+    from sovereign_moe_b200.workloads import serving_stream
+    stream = serving_stream(seed=0, count=args.count, rate=args.rate, max_rows=args.max_rows)
+    items = [(t, k.problem) for t, k in stream]
+    with Server(max_slots=args.slots) as srv:
+        done, st = srv.serve(items)
+    one, st1 = serve_one_at_a_time(items)
+    bad = [r.rid for r, (t, k) in zip(done, stream)
+           if abs(r.solution.objective - k.f_star) / max(1.0, abs(k.f_star)) > 1e-6]
+    print(json.dumps({"metric": "served LP solves/s at rel KKT 1e-6", "value": st.solves_per_s,
+                      "unit": "solves/s", "latency_s": latency_summary(st.latencies),
+                      "one_at_a_time": {"value": st1.solves_per_s,
+                                        "latency_s": latency_summary(st1.latencies)},
+                      "speedup_vs_one_at_a_time": st.solves_per_s / max(st1.solves_per_s, 1e-12),
+                      "max_concurrent": st.max_concurrent, "wrong": bad,
+                      "config": {"workload": "poisson_mixture", "rate_per_s": args.rate,
+                                 "count": args.count, "max_rows": args.max_rows}}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -425,11 +516,27 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0,
                     help="seconds of CPU work per timed CPU sample")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="batch",
+                    choices=["batch", "blend", "powerlaw", "serving"],
+                    help="batch: the headline metric; the others print auxiliary lines")
+    ap.add_argument("--iters", type=int, default=2000)
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--time-limit", type=float, default=600.0)
+    ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--count", type=int, default=200)
+    ap.add_argument("--slots", type=int, default=128)
+    ap.add_argument("--max-rows", type=int, default=None)
     args = ap.parse_args()
+    if args.workload == "blend":
+        return run_blend(args)
+    if args.workload == "powerlaw":
+        return run_powerlaw(args)
+    if args.workload == "serving":
+        return run_serving(args)
     if args.warmup < 3 and args.impl == "ours":
         ap.error("--warmup must be >= 3")
     rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.impl == "ours" else 1)))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
     return run_gpu(args, rank, world)

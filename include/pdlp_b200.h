@@ -60,6 +60,13 @@ extern "C" {
 #define PDLP_SCALING_RUIZ            2   /* Ruiz (20), pow2                     */
 #define PDLP_SCALING_POCK_CHAMBOLLE  3
 
+/* arithmetic of the iteration's sparse products (the reference: float64) */
+#define PDLP_PRECISION_FP64          0   /* everything float64                  */
+#define PDLP_PRECISION_FP32_SPMV     1   /* A x / A'y of the iteration in float32
+                                            (values, gathered directions and the
+                                            row sums); iterates, running sums,
+                                            KKT, restarts and objective float64 */
+
 /* One LP in the reference's row-bounds form rl <= Ax <= ru, l <= x <= u
  * (src/sovopt/core/problem.py:81-128).  Infinite bounds are +-1e30. */
 typedef struct pdlp_problem_desc {
@@ -94,6 +101,7 @@ typedef struct pdlp_params {
     double time_used;                   /* seconds already spent by the caller
                                            (counts against time_limit)       */
     int32_t history_capacity;           /* checks recorded (0 = none)        */
+    int32_t precision;                  /* PDLP_PRECISION_*                  */
 } pdlp_params;
 
 void pdlp_params_default(pdlp_params* p);

@@ -28,6 +28,7 @@ PDLP_STATUS_RUNNING = -1
 PDLP_SLOT_FREE = -2
 
 SCALING = {"pdlp": 0, "none": 1, "ruiz": 2, "pock_chambolle": 3}
+PRECISION = {"fp64": 0, "fp32": 1}
 
 _c_p = ctypes.c_void_p
 
@@ -50,7 +51,7 @@ class Params(ctypes.Structure):
                 ("beta_necessary", ctypes.c_double), ("beta_artificial", ctypes.c_double),
                 ("primal_weight_smoothing", ctypes.c_double), ("scaling", ctypes.c_int32),
                 ("power_start", _c_p), ("time_used", ctypes.c_double),
-                ("history_capacity", ctypes.c_int32)]
+                ("history_capacity", ctypes.c_int32), ("precision", ctypes.c_int32)]
 
 
 class Result(ctypes.Structure):

@@ -130,30 +130,58 @@ __global__ void __launch_bounds__(kBlock, 3) engine_pass(EngineArgs A, int side)
 
 // ---- admission kernels ----------------------------------------------------------
 
-// int64 compressed pointers -> int32, with structural checks.
-__global__ void convert_pointers(const long long* src, int* dst, int n, long long nnz, int* err) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i > n) return;
-  long long v = src[i];
-  if (v < 0 || v > nnz || (i == 0 && v != 0) || (i == n && v != nnz) ||
-      (i < n && src[i + 1] < v))
-    atomicOr(err, 1);
-  dst[i] = (int)v;
-}
+// All admission checks and the pointer conversions in one launch: task
+// blockIdx.y walks one array with a grid-stride loop.
+struct AdmitTasks {
+  const long long* rp64; int* rp32; int m;
+  const long long* cp64; int* cp32; int n;
+  const int* ri; const int* ci; long long nnz;
+  const double* rx0; const double* cx0;
+  const double* c0; const double* lo0; const double* hi0;
+  const double* rl0; const double* ru0;
+  int* err;
+};
 
-__global__ void check_indices(const int* idx, long long nnz, int bound, int* err) {
-  long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  for (; p < nnz; p += (long long)gridDim.x * blockDim.x) {
-    int v = idx[p];
-    if (v < 0 || v >= bound) atomicOr(err, 1);
-  }
-}
-
-__global__ void check_finite(const double* a, long long n, int allow_inf, int* err) {
-  long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  for (; p < n; p += (long long)gridDim.x * blockDim.x) {
-    double v = a[p];
-    if (isnan(v) || (!allow_inf && isinf(v))) atomicOr(err, 2);
+__global__ void admission_check(AdmitTasks T) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  switch (blockIdx.y) {
+    case 0:
+    case 1: {
+      const long long* src = blockIdx.y == 0 ? T.rp64 : T.cp64;
+      int* dst = blockIdx.y == 0 ? T.rp32 : T.cp32;
+      const int len = blockIdx.y == 0 ? T.m : T.n;
+      for (long long i = first; i <= len; i += stride) {
+        const long long v = src[i];
+        if (v < 0 || v > T.nnz || (i == 0 && v != 0) || (i == len && v != T.nnz) ||
+            (i < len && src[i + 1] < v))
+          atomicOr(T.err, 1);
+        dst[i] = (int)v;
+      }
+      break;
+    }
+    case 2:
+    case 3: {
+      const int* idx = blockIdx.y == 2 ? T.ri : T.ci;
+      const int bound = blockIdx.y == 2 ? T.n : T.m;
+      for (long long p = first; p < T.nnz; p += stride) {
+        const int v = idx[p];
+        if (v < 0 || v >= bound) atomicOr(T.err, 1);
+      }
+      break;
+    }
+    default: {
+      const int k = blockIdx.y - 4;
+      const double* a = k == 0 ? T.rx0 : k == 1 ? T.cx0 : k == 2 ? T.c0 : k == 3 ? T.lo0
+                      : k == 4 ? T.hi0 : k == 5 ? T.rl0 : T.ru0;
+      const long long len = k <= 1 ? T.nnz : (k <= 4 ? T.n : T.m);
+      const bool allow_inf = k >= 3;          // bounds may be +-inf; values and costs not
+      for (long long i = first; i < len; i += stride) {
+        const double v = a[i];
+        if (isnan(v) || (!allow_inf && isinf(v))) atomicOr(T.err, 2);
+      }
+      break;
+    }
   }
 }
 
@@ -306,10 +334,11 @@ struct SlotLayout {
   size_t mvec[14];   // c-side... see fill
   size_t nvec[16];
   size_t hist;
+  size_t rx32, cx32, dx32, dy32;
   size_t total;
 };
 
-SlotLayout layout_for(int m, int n, long long nnz, bool kind, bool v0, int hist_cap) {
+SlotLayout layout_for(int m, int n, long long nnz, bool kind, bool v0, int hist_cap, bool f32 = false) {
   Layout L;
   SlotLayout s{};
   s.rp32 = L.take(sizeof(int) * (size_t)(m + 1));
@@ -322,7 +351,7 @@ SlotLayout layout_for(int m, int n, long long nnz, bool kind, bool v0, int hist_
   s.cx = L.take(sizeof(double) * (size_t)nnz);
   s.kind = kind ? L.take((size_t)n) : 0;
   s.v0 = v0 ? L.take(sizeof(double) * (size_t)n) : 0;
-  s.tmp64 = L.take(sizeof(long long) * (size_t)(std::max(m, n) + 1));
+  s.tmp64 = L.take(sizeof(long long) * (size_t)(m + 1 + n + 1));
   s.c0 = L.take(sizeof(double) * (size_t)n);
   s.lo0 = L.take(sizeof(double) * (size_t)n);
   s.hi0 = L.take(sizeof(double) * (size_t)n);
@@ -331,6 +360,12 @@ SlotLayout layout_for(int m, int n, long long nnz, bool kind, bool v0, int hist_
   for (int i = 0; i < 14; ++i) s.mvec[i] = L.take(sizeof(double) * (size_t)m);
   for (int i = 0; i < 16; ++i) s.nvec[i] = L.take(sizeof(double) * (size_t)n);
   s.hist = L.take(sizeof(double) * 5 * (size_t)std::max(hist_cap, 0));
+  if (f32) {
+    s.rx32 = L.take(sizeof(float) * (size_t)nnz);
+    s.cx32 = L.take(sizeof(float) * (size_t)nnz);
+    s.dx32 = L.take(sizeof(float) * (size_t)n);
+    s.dy32 = L.take(sizeof(float) * (size_t)m);
+  }
   L.take(256);     // 16-byte staging copies may read a few bytes past the last array
   s.total = L.off;
   return s;
@@ -588,6 +623,8 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
   if (prm.check_every <= 0 || prm.stepsize_every <= 0) return fail(PDLP_ERR_ARG, "check_every and stepsize_every must be positive");
   if (prm.max_iter < 0) return fail(PDLP_ERR_ARG, "max_iter must be >= 0");
   if (prm.scaling < 0 || prm.scaling > 3) return fail(PDLP_ERR_ARG, "unknown scaling method");
+  if (prm.precision != PDLP_PRECISION_FP64 && prm.precision != PDLP_PRECISION_FP32_SPMV)
+    return fail(PDLP_ERR_ARG, "unknown precision");
   if (!std::isfinite(P->obj_offset)) return fail(PDLP_ERR_NUMERICAL, "obj_offset is not finite");
   int slot = -1;
   for (size_t s = 0; s < b->slots.size(); ++s) if (!b->slots[s].used) { slot = (int)s; break; }
@@ -617,7 +654,8 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
   const int hist_cap = std::max(0, prm.history_capacity);
   const bool has_kind = P->kind != nullptr;
   const bool has_v0 = prm.power_start != nullptr;
-  SlotLayout L = layout_for(m, n, nnz, has_kind, has_v0, hist_cap);
+  const bool f32 = prm.precision == PDLP_PRECISION_FP32_SPMV;
+  SlotLayout L = layout_for(m, n, nnz, has_kind, has_v0, hist_cap, f32);
   size_t budget = (size_t)b->cfg.memory_budget;
   if (budget == 0) {
     size_t fr = 0, tot = 0;
@@ -644,10 +682,10 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
   // the state's error word doubles as the validation flag
   int* err_flag = &b->d_state[slot].error;
   PDLP_CUDA(cudaMemsetAsync(&b->d_state[slot], 0, sizeof(State), st));
-  if ((rc = copy_in(at(L.tmp64), P->rp, sizeof(int64_t) * (m + 1), mem, st))) return cleanup(rc);
-  convert_pointers<<<(m + 256) / 256, 256, 0, st>>>((const long long*)at(L.tmp64), (int*)at(L.rp32), m, nnz, err_flag);
-  if ((rc = copy_in(at(L.tmp64), P->cp, sizeof(int64_t) * (n + 1), mem, st))) return cleanup(rc);
-  convert_pointers<<<(n + 256) / 256, 256, 0, st>>>((const long long*)at(L.tmp64), (int*)at(L.cp32), n, nnz, err_flag);
+  long long* rp64 = (long long*)at(L.tmp64);
+  long long* cp64 = rp64 + (m + 1);
+  if ((rc = copy_in(rp64, P->rp, sizeof(int64_t) * (m + 1), mem, st))) return cleanup(rc);
+  if ((rc = copy_in(cp64, P->cp, sizeof(int64_t) * (n + 1), mem, st))) return cleanup(rc);
   if ((rc = copy_in(at(L.ri), P->ri, sizeof(int) * nnz, mem, st))) return cleanup(rc);
   if ((rc = copy_in(at(L.ci), P->ci, sizeof(int) * nnz, mem, st))) return cleanup(rc);
   if ((rc = copy_in(at(L.rx0), P->rx, sizeof(double) * nnz, mem, st))) return cleanup(rc);
@@ -659,23 +697,21 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
   if ((rc = copy_in(at(L.ru0), P->row_ub, sizeof(double) * m, mem, st))) return cleanup(rc);
   if (has_kind && (rc = copy_in(at(L.kind), P->kind, (size_t)n, mem, st))) return cleanup(rc);
   if (has_v0 && (rc = copy_in(at(L.v0), prm.power_start, sizeof(double) * n, mem, st))) return cleanup(rc);
-  auto grid_for = [](long long cnt) { return (int)std::max(1LL, std::min(4096LL, (cnt + 255) / 256)); };
-  if (nnz > 0) {
-    check_indices<<<grid_for(nnz), 256, 0, st>>>((const int*)at(L.ri), nnz, n, err_flag);
-    check_indices<<<grid_for(nnz), 256, 0, st>>>((const int*)at(L.ci), nnz, m, err_flag);
-    check_finite<<<grid_for(nnz), 256, 0, st>>>((const double*)at(L.rx0), nnz, 0, err_flag);
-    check_finite<<<grid_for(nnz), 256, 0, st>>>((const double*)at(L.cx0), nnz, 0, err_flag);
+  {
+    AdmitTasks T;
+    T.rp64 = rp64; T.rp32 = (int*)at(L.rp32); T.m = m;
+    T.cp64 = cp64; T.cp32 = (int*)at(L.cp32); T.n = n;
+    T.ri = (const int*)at(L.ri); T.ci = (const int*)at(L.ci); T.nnz = nnz;
+    T.rx0 = (const double*)at(L.rx0); T.cx0 = (const double*)at(L.cx0);
+    T.c0 = (const double*)at(L.c0); T.lo0 = (const double*)at(L.lo0); T.hi0 = (const double*)at(L.hi0);
+    T.rl0 = (const double*)at(L.rl0); T.ru0 = (const double*)at(L.ru0);
+    T.err = err_flag;
+    const long long most = std::max<long long>({nnz, (long long)m + 1, (long long)n + 1});
+    const int gx = (int)std::max(1LL, std::min(1024LL, (most + 255) / 256));
+    admission_check<<<dim3(gx, 11), 256, 0, st>>>(T);
+    PDLP_CUDA(cudaGetLastError());
+    count_launches(1);
   }
-  if (n > 0) {
-    check_finite<<<grid_for(n), 256, 0, st>>>((const double*)at(L.c0), n, 0, err_flag);
-    check_finite<<<grid_for(n), 256, 0, st>>>((const double*)at(L.lo0), n, 1, err_flag);
-    check_finite<<<grid_for(n), 256, 0, st>>>((const double*)at(L.hi0), n, 1, err_flag);
-  }
-  if (m > 0) {
-    check_finite<<<grid_for(m), 256, 0, st>>>((const double*)at(L.rl0), m, 1, err_flag);
-    check_finite<<<grid_for(m), 256, 0, st>>>((const double*)at(L.ru0), m, 1, err_flag);
-  }
-  count_launches(2 + (nnz > 0 ? 4 : 0) + (n > 0 ? 3 : 0) + (m > 0 ? 2 : 0));
   int herr = 0;
   PDLP_CUDA(cudaMemcpyAsync(&herr, err_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
   e = cudaStreamSynchronize(st);
@@ -714,6 +750,11 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
                      &I.xbar, &I.atybar, &I.atyf, &I.xrst, &I.xout, &I.dout, nullptr};
   for (int i = 0; i < 15; ++i) *nv[i] = (double*)at(L.nvec[i]);
   I.v0 = has_v0 ? (const double*)at(L.v0) : nullptr;
+  I.f32 = f32 ? 1 : 0;
+  I.rx32 = f32 ? (float*)at(L.rx32) : nullptr;
+  I.cx32 = f32 ? (float*)at(L.cx32) : nullptr;
+  I.dx32 = f32 ? (float*)at(L.dx32) : nullptr;
+  I.dy32 = f32 ? (float*)at(L.dy32) : nullptr;
   I.hist = hist_cap ? (double*)at(L.hist) : nullptr;
   I.hist_cap = hist_cap;
   I.eps_abs = prm.eps_abs; I.eps_rel = prm.eps_rel; I.feas_cap = prm.feas_cap;
@@ -725,7 +766,13 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
   I.theta = prm.primal_weight_smoothing;
   plan_tiles(rp, m, slot, b->cfg.tile_rows, b->cfg.tile_nnz, S.rt, S.rtw);
   plan_tiles(cp, n, slot, b->cfg.tile_rows, b->cfg.tile_nnz, S.ct, S.ctw);
-  S.bytes_per_iter = 24.0 * (double)nnz + 4.0 * (m + 1) + 4.0 * (n + 1) + 8.0 * (10.0 * m + 11.0 * n);
+  // algorithmic bytes of one PDHG iteration: value + index per
+  // entry and pointer per row on both passes, one gathered word per column /
+  // row, the vectors each pass reads and writes
+  S.bytes_per_iter = f32 ? 16.0 * (double)nnz + 4.0 * (m + 1) + 4.0 * (n + 1) +
+                               4.0 * (m + n) + 8.0 * (9.0 * m + 10.0 * n) + 4.0 * (m + n)
+                         : 24.0 * (double)nnz + 4.0 * (m + 1) + 4.0 * (n + 1) +
+                               8.0 * (10.0 * m + 11.0 * n);
 
   init.status = PDLP_STATUS_RUNNING;
   init.final_status = PDLP_STATUS_RUNNING;

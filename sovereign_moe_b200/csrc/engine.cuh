@@ -88,6 +88,9 @@ struct Inst {
   // column-side vectors (length n)
   double *x, *aty, *dx, *xnew, *sumx, *xbar, *atybar, *atyf, *xrst, *xout, *dout;
   const double* v0;                         // power-iteration start, or null
+  int f32;                                  // 1: iteration SpMVs in float32
+  float* rx32; float* cx32;                 // float32 scaled values (f32 only)
+  float* dx32; float* dy32;                 // float32 copies of dx, dy (f32 only)
   double* hist;
   int hist_cap;
   // parameters (pdlp.py:79-116)

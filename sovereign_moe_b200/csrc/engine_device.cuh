@@ -196,6 +196,34 @@ __device__ __forceinline__ void staged_row_sums(const int* tptr, const double* p
   __syncwarp();
 }
 
+// The same in float32 (FP32-SpMV precision): products in float, each row's
+// sum accumulated in float in storage order, written out as double.
+__device__ __forceinline__ void staged_row_sums_f32(const int* tptr, const float* prod, int rows,
+                                                    int L, double* out, int lane) {
+  const int p0 = tptr[0];
+  const int sub = lane & (L - 1);
+  const int grp = lane / L, ngrp = 32 / L;
+  for (int rb = 0; rb < rows; rb += ngrp) {
+    const int li = rb + grp;
+    float a = 0.0f;
+    if (li < rows) {
+      const int e = tptr[li + 1] - p0;
+      int q = tptr[li] - p0 + sub;
+      for (; q + 7 * L < e; q += 8 * L) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = prod[q + u * L];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) a += v[u];
+      }
+      for (; q < e; q += L) a += prod[q];
+    }
+    for (int off = L >> 1; off > 0; off >>= 1) a += __shfl_xor_sync(kFull, a, off);
+    if (li < rows && sub == 0) out[li] = (double)a;
+  }
+  __syncwarp();
+}
+
 // Per-row max of f(r, p) over the tile (Ruiz pass); result in W.s0.
 template <class F>
 __device__ __forceinline__ void warp_rowmax(const Tile& t, const int* ptr, int L, F f,

@@ -204,6 +204,25 @@ __device__ __forceinline__ void gather_products(const Tile& t, const double* src
   __syncwarp();
 }
 
+__device__ __forceinline__ void gather_products_f32(const Tile& t, const float* src, WarpSmem& W,
+                                                    int offi, int offv, int lane) {
+  float* prod = reinterpret_cast<float*>(W.sval) + offv;
+  const int* idx = W.sidx + offi;
+  const int cnt = t.cnt;
+  float g[kWTileNnz / 32];
+#pragma unroll
+  for (int u = 0; u < kWTileNnz / 32; ++u) {
+    const int q = lane + 32 * u;
+    g[u] = q < cnt ? __ldcg(src + idx[q]) : 0.0f;
+  }
+#pragma unroll
+  for (int u = 0; u < kWTileNnz / 32; ++u) {
+    const int q = lane + 32 * u;
+    if (q < cnt) prod[q] *= g[u];
+  }
+  __syncwarp();
+}
+
 __device__ void hot_rtile(const EngineArgs& A, const Tile& t, int ti, const Inst& I, State* S,
                           WarpSmem& W, int lane, int rmode, bool commit, double eta,
                           double omega, int offp, int offi, int offv) {
@@ -235,9 +254,16 @@ __device__ void hot_rtile(const EngineArgs& A, const Tile& t, int ti, const Inst
   cp_async_wait<1>();
   __syncwarp();
   HOT_STAMP(2);
-  gather_products(t, I.dx, W, offi, offv, lane);
-  HOT_STAMP(3);
-  staged_row_sums(W.sptr + offp, W.sval + offv, rows, I.lanes_r, W.s0, lane);
+  if (I.f32) {
+    gather_products_f32(t, I.dx32, W, offi, offv, lane);
+    HOT_STAMP(3);
+    staged_row_sums_f32(W.sptr + offp, reinterpret_cast<const float*>(W.sval) + offv, rows,
+                        I.lanes_r, W.s0, lane);
+  } else {
+    gather_products(t, I.dx, W, offi, offv, lane);
+    HOT_STAMP(3);
+    staged_row_sums(W.sptr + offp, W.sval + offv, rows, I.lanes_r, W.s0, lane);
+  }
   HOT_STAMP(4);
   cp_async_wait<0>();
   __syncwarp();
@@ -266,6 +292,7 @@ __device__ void hot_rtile(const EngineArgs& A, const Tile& t, int ti, const Inst
       const double w = y + sigma * (axn + a);
       const double yn = prox(w, sigma, rl, ru);
       I.dy[r] = yn - y;
+      if (I.f32) I.dy32[r] = (float)(yn - y);
       I.y[r] = yn;
       I.sumy[r] = sumy + eta * yn;
     } else {                          // pdlp.py:347-356
@@ -276,6 +303,7 @@ __device__ void hot_rtile(const EngineArgs& A, const Tile& t, int ti, const Inst
       I.ynew[r] = yn;
       const double d = yn - y;
       I.dy[r] = d;
+      if (I.f32) I.dy32[r] = (float)d;
       acc[0] += d * a;
       acc[1] += d * d;
     }
@@ -321,8 +349,14 @@ __device__ void hot_ctile(const EngineArgs& A, const Tile& t, int ti, const Inst
   if (iter) {
     cp_async_wait<1>();
     __syncwarp();
-    gather_products(t, I.dy, W, offi, offv, lane);
-    staged_row_sums(W.sptr + offp, W.sval + offv, rows, I.lanes_c, W.s0, lane);
+    if (I.f32) {
+      gather_products_f32(t, I.dy32, W, offi, offv, lane);
+      staged_row_sums_f32(W.sptr + offp, reinterpret_cast<const float*>(W.sval) + offv, rows,
+                          I.lanes_c, W.s0, lane);
+    } else {
+      gather_products(t, I.dy, W, offi, offv, lane);
+      staged_row_sums(W.sptr + offp, W.sval + offv, rows, I.lanes_c, W.s0, lane);
+    }
   }
   cp_async_wait<0>();
   __syncwarp();
@@ -345,6 +379,7 @@ __device__ void hot_ctile(const EngineArgs& A, const Tile& t, int ti, const Inst
       const double xn = clip(xv - tau * (W.vec[2][v] + atyv), W.vec[3][v], W.vec[4][v]);
       const double d = xn - xv;
       I.dx[j] = d;
+      if (I.f32) I.dx32[j] = (float)d;
       if (cprimal == P_TRIAL) {
         I.xnew[j] = xn;
         if (xc) I.x[j] = xv;
@@ -386,7 +421,8 @@ __device__ void process_rtile(const EngineArgs& A, const Tile t, int ti, WarpSme
   if (!t.heavy) {
     offp = stage<4>(W.sptr, I.rp, t.begin, t.end - t.begin + 1, lane);
     offi = stage<4>(W.sidx, I.ri, t.p0, t.cnt, lane);
-    offv = stage<8>(W.sval, I.rx, t.p0, t.cnt, lane);
+    offv = I.f32 ? stage<4>(W.sval, I.rx32, t.p0, t.cnt, lane)
+                 : stage<8>(W.sval, I.rx, t.p0, t.cnt, lane);
   }
   cp_async_commit();
   const int rmode = ld_mut(&S->rmode);
@@ -485,7 +521,9 @@ __device__ void process_rtile(const EngineArgs& A, const Tile t, int ti, WarpSme
     }
     case R_APPLY: {
       warp_entries(t, rp, [&](int r, int p) {
-        I.rx[p] = ld_ro(I.rx0 + p) * (ld_mut(I.rs + r) * ld_mut(I.cs + ld_ro(ri + p)));
+        const double v = ld_ro(I.rx0 + p) * (ld_mut(I.rs + r) * ld_mut(I.cs + ld_ro(ri + p)));
+        I.rx[p] = v;
+        if (I.f32) I.rx32[p] = (float)v;
       }, lane);
       ops.maxmask = 1u;
       for (int r = t.begin + lane; r < rend; r += 32) {
@@ -503,6 +541,7 @@ __device__ void process_rtile(const EngineArgs& A, const Tile t, int ti, WarpSme
     case R_SETUP0: {
       for (int r = t.begin + lane; r < rend; r += 32) {
         I.y[r] = 0.0; I.sumy[r] = 0.0; I.yrst[r] = 0.0; I.dy[r] = 0.0;
+        if (I.f32) I.dy32[r] = 0.0f;
       }
       break;
     }
@@ -547,6 +586,7 @@ __device__ void process_rtile(const EngineArgs& A, const Tile t, int ti, WarpSme
         const double w = yo + sigma * (axn + a);
         const double yn = prox(w, sigma, ld_mut(I.rl + r), ld_mut(I.ru + r));
         I.dy[r] = yn - yo;
+        if (I.f32) I.dy32[r] = (float)(yn - yo);
         I.y[r] = yn;
         I.sumy[r] = ld_mut(I.sumy + r) + eta * yn;
       }
@@ -570,6 +610,7 @@ __device__ void process_rtile(const EngineArgs& A, const Tile t, int ti, WarpSme
         I.ynew[r] = yn;
         const double d = yn - yo;
         I.dy[r] = d;
+        if (I.f32) I.dy32[r] = (float)d;
         acc[0] += d * a;
         acc[1] += d * d;
       }
@@ -670,6 +711,7 @@ __device__ __forceinline__ double primal_half(const Inst& I, int j, double xv, d
   const double xn = clip(xv - tau * (ld_mut(I.c + j) + atyv), l, h);
   const double d = xn - xv;
   I.dx[j] = d;
+  if (I.f32) I.dx32[j] = (float)d;
   if (kind == P_TRIAL) {
     I.xnew[j] = xn;
     if (wrote_x) I.x[j] = xv;
@@ -864,7 +906,8 @@ __device__ void process_ctile(const EngineArgs& A, const Tile t, int ti, WarpSme
   if (!t.heavy) {
     offp = stage<4>(W.sptr, I.cp, t.begin, t.end - t.begin + 1, lane);
     offi = stage<4>(W.sidx, I.ci, t.p0, t.cnt, lane);
-    offv = stage<8>(W.sval, I.cx, t.p0, t.cnt, lane);
+    offv = I.f32 ? stage<4>(W.sval, I.cx32, t.p0, t.cnt, lane)
+                 : stage<8>(W.sval, I.cx, t.p0, t.cnt, lane);
   }
   cp_async_commit();
   const int cmode = ld_mut(&S->cmode);
@@ -952,7 +995,9 @@ __device__ void process_ctile(const EngineArgs& A, const Tile t, int ti, WarpSme
     }
     case C_APPLY: {
       warp_entries(t, cp, [&](int j, int p) {
-        I.cx[p] = ld_ro(I.cx0 + p) * (ld_mut(I.rs + ld_ro(ci + p)) * ld_mut(I.cs + j));
+        const double v = ld_ro(I.cx0 + p) * (ld_mut(I.rs + ld_ro(ci + p)) * ld_mut(I.cs + j));
+        I.cx[p] = v;
+        if (I.f32) I.cx32[p] = (float)v;
       }, lane);
       ops.maxmask = 5u;       // slots 0 and 2
       ops.minmask = 2u;       // slot 1
@@ -982,6 +1027,7 @@ __device__ void process_ctile(const EngineArgs& A, const Tile t, int ti, WarpSme
         const double l = ld_mut(I.lo + j), h = ld_mut(I.hi + j);
         const double x0 = clip(0.0, l, h);
         I.x[j] = x0; I.xrst[j] = x0; I.aty[j] = 0.0; I.sumx[j] = 0.0; I.dx[j] = 0.0;
+        if (I.f32) I.dx32[j] = 0.0f;
         const double v0 = I.v0 != nullptr ? ld_ro(I.v0 + j)
                                           : gen_normal((unsigned long long)j);
         I.xbar[j] = v0;

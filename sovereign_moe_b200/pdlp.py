@@ -47,6 +47,10 @@ class PDLPParams:
     device: str = "auto"
     verbose: bool = False
     log_every: int = 2000
+    # B200 engine only (not in the reference): arithmetic of the iteration's
+    # sparse products, "fp64" (the reference's) or "fp32" (float32 values,
+    # directions and row sums; iterates and every check stay float64)
+    precision: str = "fp64"
 
 
 @dataclass
@@ -117,6 +121,10 @@ def params_struct(params: PDLPParams, n: int, time_used: float = 0.0, history_ca
     p.beta_artificial = params.beta_artificial
     p.primal_weight_smoothing = params.primal_weight_smoothing
     p.scaling = _lib.SCALING[params.scaling]
+    prec = getattr(params, "precision", "fp64")
+    if prec not in _lib.PRECISION:
+        raise ValueError(f"unknown precision {prec!r}; choose from {sorted(_lib.PRECISION)}")
+    p.precision = _lib.PRECISION[prec]
     p.time_used = float(time_used)
     if history_capacity is None:
         history_capacity = int(min(params.max_iter // max(params.check_every, 1) + 1, 1 << 20))

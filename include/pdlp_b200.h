@@ -222,6 +222,21 @@ int pdlp_pdhg_accum(int32_t n, double* acc, const double* inc, double* run_sum,
 int pdlp_dot(int64_t n, const double* a, const double* b, double* out, void* stream);
 int pdlp_nrm2(int64_t n, const double* a, double* out, void* stream);
 int pdlp_nrm_inf(int64_t n, const double* a, double* out, void* stream);
+/* a . b to a host double, like pdlp_dot, but without allocating any device
+ * memory.  No counterpart in the reference.  It is for callers that must not
+ * allocate: a serving loop that has given the free device memory to resident
+ * problems (an allocation there could fail with out-of-memory in the middle
+ * of a step), or any caller whose device footprint must stay fixed and known
+ * before it starts.  The scratch is one fixed 128 KiB array per device, so n
+ * is limited to 2^28 = 268435456 elements; a larger n returns PDLP_ERR_ARG
+ * (use pdlp_dot then).  The first call on a device (n = 0 is enough) looks up
+ * that array's address with the device current: make it before any stream
+ * capture.  Every call on a device shares the array and leaves the last
+ * call's partial sums in it, so calls whose execution overlaps (other
+ * streams, other host threads) race and must be serialised by the caller.
+ * The result equals pdlp_dot's up to rounding (a different, but fixed,
+ * summation tree). */
+int pdlp_dot_noalloc(int64_t n, const double* a, const double* b, double* out, void* stream);
 
 #ifdef __cplusplus
 }

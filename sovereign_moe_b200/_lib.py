@@ -106,6 +106,7 @@ SIGNATURES = {
     "pdlp_dot": ([_i64, _c_p, _c_p, ctypes.POINTER(_d), _c_p], ctypes.c_int),
     "pdlp_nrm2": ([_i64, _c_p, ctypes.POINTER(_d), _c_p], ctypes.c_int),
     "pdlp_nrm_inf": ([_i64, _c_p, ctypes.POINTER(_d), _c_p], ctypes.c_int),
+    "pdlp_dot_noalloc": ([_i64, _c_p, _c_p, ctypes.POINTER(_d), _c_p], ctypes.c_int),
 }
 
 _LIB = None

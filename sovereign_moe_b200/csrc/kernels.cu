@@ -3,6 +3,8 @@
 // step kernels and the reductions, on device pointers and a caller stream.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <string>
 
 #include "common.cuh"
 
@@ -208,6 +210,67 @@ int reduce(long long n, const double* a, const double* b, int op, double* out, c
   return PDLP_OK;
 }
 
+// ---- dot product with a fixed, statically allocated scratch ---------------
+// pdlp_dot_noalloc serves callers that must not allocate device memory (a
+// serving loop whose free memory is held by resident problems, a caller with
+// a fixed device footprint).  It reduces chunks of kNaChunk elements, one
+// block per chunk, into the partials at the head of noalloc_scratch; the
+// final block sum goes to the slot after the largest partial count.  The
+// array is one per device, 128 KiB, shared by every call on that device and
+// left holding the last call's sums: calls that overlap in time race.
+constexpr int kNaChunk = 16384;
+constexpr int kNaMaxChunks = 16384;
+constexpr long long kNaMaxN = (long long)kNaChunk * kNaMaxChunks;   // 2^28 elements
+constexpr int kNaMaxDevices = 64;
+static __device__ __align__(256) double noalloc_scratch[kNaMaxChunks + 1];
+
+// partials[blockIdx.x] = sum of a[i] * b[i] over the block's chunk, in a fixed
+// order (thread t takes elements t, t + kT, ... of the chunk; warp and block
+// trees after), so repeated calls give the same bits.
+__global__ void __launch_bounds__(kT) dot_chunk_kernel(long long n, const double* __restrict__ a,
+                                                       const double* __restrict__ b,
+                                                       double* __restrict__ partials) {
+  __shared__ double sh[kT / 32];
+  const long long base = (long long)blockIdx.x * kNaChunk;
+  const long long end = min(n, base + kNaChunk);
+  double acc = 0.0;
+#pragma unroll 8
+  for (long long i = base + threadIdx.x; i < end; i += kT) acc += a[i] * b[i];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(kAll, acc, off);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (kT / 32) ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(kAll, v, off);
+    if (threadIdx.x == 0) partials[blockIdx.x] = v;
+  }
+}
+
+// Device address of noalloc_scratch, looked up once per device ordinal (with
+// that device current) on the first call made there.
+std::mutex noalloc_mu;
+double* noalloc_ptr[kNaMaxDevices] = {};
+
+int noalloc_scratch_ptr(double** out) {
+  int dev = 0;
+  PDLP_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNaMaxDevices)
+    return fail(PDLP_ERR_ARG, "pdlp_dot_noalloc: device ordinal " + std::to_string(dev) +
+                                  " is beyond the " + std::to_string(kNaMaxDevices) +
+                                  " devices it supports");
+  std::lock_guard<std::mutex> lock(noalloc_mu);
+  if (!noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(noalloc_scratch)");
+    noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = noalloc_ptr[dev];
+  return PDLP_OK;
+}
+
 }  // namespace
 }  // namespace pdlp
 
@@ -298,6 +361,35 @@ int pdlp_nrm2(int64_t n, const double* a, double* out, void* stream) {
 
 int pdlp_nrm_inf(int64_t n, const double* a, double* out, void* stream) {
   return reduce(n, a, nullptr, RED_ABSMAX, out, (cudaStream_t)stream);
+}
+
+int pdlp_dot_noalloc(int64_t n, const double* a, const double* b, double* out, void* stream) {
+  if (!out) return fail(PDLP_ERR_ARG, "out is NULL");
+  if (n < 0) return fail(PDLP_ERR_ARG, "n must be >= 0");
+  if (n > kNaMaxN)
+    return fail(PDLP_ERR_ARG, "pdlp_dot_noalloc: n = " + std::to_string((long long)n) +
+                                  " is above its fixed-scratch limit of " +
+                                  std::to_string(kNaMaxN) + " elements; use pdlp_dot");
+  double* scratch = nullptr;
+  const int rc = noalloc_scratch_ptr(&scratch);
+  if (rc != PDLP_OK) return rc;
+  if (n == 0) { *out = 0.0; return PDLP_OK; }
+  if (!a || !b) return fail(PDLP_ERR_ARG, "NULL pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  // every partial the final sum reads is written by this call first: nothing
+  // in the scratch has to start at zero
+  const int chunks = (int)((n + kNaChunk - 1) / kNaChunk);
+  dot_chunk_kernel<<<chunks, kT, 0, st>>>(n, a, b, scratch);
+  reduce_final_kernel<<<1, kT, 0, st>>>(chunks, scratch, RED_DOT, scratch + kNaMaxChunks);
+  count_launches(2);
+  cudaError_t e = cudaGetLastError();
+  double h = 0.0;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&h, scratch + kNaMaxChunks, sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "pdlp_dot_noalloc");
+  *out = h;
+  return PDLP_OK;
 }
 
 }  // extern "C"

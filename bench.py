@@ -485,6 +485,34 @@ def run_powerlaw(args):
     return 0
 
 
+def run_engine_steps(args):
+    """A bounded run of the engine kernel on the headline batch (256 LPs of
+    uneven size): admit, run ``--iters`` engine steps in launches of at most
+    256 steps (the first launch includes scaling and set-up), report each
+    launch.  Small and short enough to capture one launch under a profiler."""
+    from sovereign_moe_b200.batch import BatchEngine
+    lps = make_batch(1000)
+    launches = []
+    with BatchEngine(max_slots=len(lps)) as eng:
+        for k in lps:
+            eng.admit(k.problem, params())
+        done = 0
+        while done < args.iters:
+            n = min(256, args.iters - done)
+            active = eng.step(n)
+            ms, by, its = eng.last_timing()
+            launches.append({"steps": n, "active_after": active, "ms": ms,
+                             "us_per_step": 1000.0 * ms / n, "iterations": its,
+                             "achieved_GBps": by / ms / 1e6 if ms else 0.0})
+            done += n
+            if active == 0:
+                break
+    print(json.dumps({"metric": "engine launches (bounded run)", "launches": launches,
+                      "config": {"workload": "uneven_batch_256", "lps": len(lps),
+                                 "steps": args.iters}}), flush=True)
+    return 0
+
+
 def run_serving(args):
     """Poisson arrivals served with continuous batching vs one at a time."""
     from sovereign_moe_b200.serving import Server, latency_summary, serve_one_at_a_time
@@ -517,7 +545,7 @@ def main():
                     help="seconds of CPU work per timed CPU sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="batch",
-                    choices=["batch", "blend", "powerlaw", "serving"],
+                    choices=["batch", "blend", "powerlaw", "serving", "engine-steps"],
                     help="batch: the headline metric; the others print auxiliary lines")
     ap.add_argument("--iters", type=int, default=2000)
     ap.add_argument("--scale", type=float, default=1.0)
@@ -533,6 +561,8 @@ def main():
         return run_powerlaw(args)
     if args.workload == "serving":
         return run_serving(args)
+    if args.workload == "engine-steps":
+        return run_engine_steps(args)
     if args.warmup < 3 and args.impl == "ours":
         ap.error("--warmup must be >= 3")
     rank = int(os.environ.get("RANK", "0"))

@@ -41,6 +41,12 @@ __device__ __forceinline__ int ld_mut(const int* p) { return __ldcg(p); }
 __device__ __forceinline__ long long ld_mut(const long long* p) { return __ldcg(p); }
 
 // Loads of data that is immutable for the whole launch.
+// Gathers of a vector that was written before the last grid barrier and is
+// not written again until the next one: L1-cached.  The barrier's acquire
+// (ld.acquire.gpu, then bar.sync) orders those writes before these loads, so
+// no stale L1 line can be returned.
+__device__ __forceinline__ double ld_gather(const double* p) { return __ldca(p); }
+__device__ __forceinline__ float ld_gather(const float* p) { return __ldca(p); }
 __device__ __forceinline__ double ld_ro(const double* p) { return __ldg(p); }
 __device__ __forceinline__ int ld_ro(const int* p) { return __ldg(p); }
 

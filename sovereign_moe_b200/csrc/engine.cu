@@ -54,7 +54,7 @@ __device__ bool grid_barrier(Control* ctl, unsigned target, long long timeout_ns
 extern __shared__ __align__(16) unsigned char g_smem[];
 constexpr size_t kSmemBytes = sizeof(WarpSmem) * kWarps + 16;
 
-__global__ void __launch_bounds__(kBlock, 3) engine_persistent(EngineArgs A) {
+__global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
   WarpSmem* ws = reinterpret_cast<WarpSmem*>(g_smem);
   int& flag = *reinterpret_cast<int*>(g_smem + sizeof(WarpSmem) * kWarps);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -86,10 +86,11 @@ __global__ void __launch_bounds__(kBlock, 3) engine_persistent(EngineArgs A) {
     PDLP_STAMP(step, 0);
     {
       Tile next = rfirst;
+      PassCache pc;
       for (int t = r0; t < r1; ++t) {
         const Tile cur = next;
         if (t + 1 < r1) next = A.rtiles[t + 1];      // prefetch the next descriptor
-        process_rtile(A, cur, t, W, lane);
+        process_rtile(A, cur, t, W, lane, pc);
       }
     }
     PDLP_STAMP(step, 1);
@@ -98,10 +99,11 @@ __global__ void __launch_bounds__(kBlock, 3) engine_persistent(EngineArgs A) {
     PDLP_STAMP(step, 2);
     {
       Tile next = cfirst;
+      PassCache pc;
       for (int t = c0; t < c1; ++t) {
         const Tile cur = next;
         if (t + 1 < c1) next = A.ctiles[t + 1];
-        process_ctile(A, cur, t, W, lane);
+        process_ctile(A, cur, t, W, lane, pc);
       }
     }
     PDLP_STAMP(step, 3);
@@ -121,10 +123,11 @@ __global__ void __launch_bounds__(kBlock, 3) engine_pass(EngineArgs A, int side)
   __syncwarp();
   const int gw = blockIdx.x * kWarps + warp;
   const int nw = gridDim.x * kWarps;
+  PassCache pc;
   if (side == 0) {
-    for (int t = gw; t < A.n_rtiles; t += nw) process_rtile(A, A.rtiles[t], t, W, lane);
+    for (int t = gw; t < A.n_rtiles; t += nw) process_rtile(A, A.rtiles[t], t, W, lane, pc);
   } else {
-    for (int t = gw; t < A.n_ctiles; t += nw) process_ctile(A, A.ctiles[t], t, W, lane);
+    for (int t = gw; t < A.n_ctiles; t += nw) process_ctile(A, A.ctiles[t], t, W, lane, pc);
   }
 }
 
@@ -269,6 +272,10 @@ struct pdlp_batch {
   std::vector<Slot> slots;
   int n_running = 0;
   size_t bytes_held = 0;
+  // arenas of retired LPs, kept for later admissions: reusing one costs no
+  // allocation and no device synchronisation (all use is stream-ordered)
+  std::vector<std::pair<void*, size_t>> spare;
+  size_t bytes_spare = 0;
   // device arrays
   Inst* d_inst = nullptr;
   State* d_state = nullptr;
@@ -538,11 +545,11 @@ int pdlp_batch_create(const pdlp_batch_config* cfg, void* stream, pdlp_batch** o
   if (cfg) c = *cfg;
   if (c.max_slots <= 0) return fail(PDLP_ERR_ARG, "max_slots must be positive");
   if (c.block_threads == 0) c.block_threads = kBlock;
-  if (c.block_threads != kBlock) return fail(PDLP_ERR_ARG, "block_threads must be 256");
+  if (c.block_threads != kBlock) return fail(PDLP_ERR_ARG, "block_threads must be " + std::to_string(kBlock));
   if (c.tile_rows <= 0) c.tile_rows = default_tile_rows();
-  if (c.tile_rows > kWTileRows) return fail(PDLP_ERR_ARG, "tile_rows exceeds 128");
+  if (c.tile_rows > kWTileRows) return fail(PDLP_ERR_ARG, "tile_rows exceeds " + std::to_string(kWTileRows));
   if (c.tile_nnz <= 0) c.tile_nnz = default_tile_nnz();
-  if (c.tile_nnz > kWTileNnz) return fail(PDLP_ERR_ARG, "tile_nnz exceeds 512");
+  if (c.tile_nnz > kWTileNnz) return fail(PDLP_ERR_ARG, "tile_nnz exceeds " + std::to_string(kWTileNnz));
   if (c.lanes_override && (c.lanes_override & (c.lanes_override - 1)))
     return fail(PDLP_ERR_ARG, "lanes_override must be a power of two");
   pdlp_batch* b = new pdlp_batch();
@@ -594,6 +601,7 @@ int pdlp_batch_destroy(pdlp_batch* b) {
   if (!b) return PDLP_OK;
   cudaStreamSynchronize(b->stream);
   for (auto& s : b->slots) if (s.arena) cudaFree(s.arena);
+  for (auto& a : b->spare) cudaFree(a.first);
   cudaFree(b->d_inst); cudaFree(b->d_state); cudaFree(b->d_counters); cudaFree(b->d_ctl);
   cudaFree(b->d_rtiles); cudaFree(b->d_ctiles); cudaFree(b->d_rwarp); cudaFree(b->d_cwarp);
   cudaFree(b->d_partials); cudaFree(b->d_group_tiles); cudaFree(b->d_gpartials);
@@ -656,24 +664,59 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
   const bool has_v0 = prm.power_start != nullptr;
   const bool f32 = prm.precision == PDLP_PRECISION_FP32_SPMV;
   SlotLayout L = layout_for(m, n, nnz, has_kind, has_v0, hist_cap, f32);
-  size_t budget = (size_t)b->cfg.memory_budget;
-  if (budget == 0) {
-    size_t fr = 0, tot = 0;
-    PDLP_CUDA(cudaMemGetInfo(&fr, &tot));
-    budget = b->bytes_held + (fr > ((size_t)1 << 30) ? fr - ((size_t)1 << 30) : 0);
+  // a retired arena that holds the layout without wasting more than half of itself
+  int best = -1;
+  for (size_t i = 0; i < b->spare.size(); ++i) {
+    const size_t sz = b->spare[i].second;
+    if (sz >= L.total && sz <= 2 * L.total + ((size_t)1 << 20) &&
+        (best < 0 || sz < b->spare[(size_t)best].second))
+      best = (int)i;
   }
-  if (b->bytes_held + L.total > budget)
-    return fail(PDLP_ERR_OOM, "admission refused: the LP does not fit the memory budget");
   void* arena = nullptr;
-  cudaError_t e = cudaMalloc(&arena, L.total);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    return fail(PDLP_ERR_OOM, std::string("admission refused: cudaMalloc: ") + cudaGetErrorString(e));
+  size_t arena_bytes = L.total;
+  cudaError_t e = cudaSuccess;
+  if (best >= 0) {
+    arena = b->spare[(size_t)best].first;
+    arena_bytes = b->spare[(size_t)best].second;
+    b->spare.erase(b->spare.begin() + best);
+    b->bytes_spare -= arena_bytes;
+  } else {
+    // a new arena: within the budget (spare arenas are released first if needed)
+    auto fits = [&](bool* ok) -> int {
+      if (b->cfg.memory_budget > 0) {
+        *ok = b->bytes_held + b->bytes_spare + L.total <= (size_t)b->cfg.memory_budget;
+      } else {
+        size_t fr = 0, tot = 0;
+        PDLP_CUDA(cudaMemGetInfo(&fr, &tot));
+        *ok = L.total <= (fr > ((size_t)1 << 30) ? fr - ((size_t)1 << 30) : 0);
+      }
+      return PDLP_OK;
+    };
+    bool ok = false;
+    int frc = fits(&ok);
+    if (frc) return frc;
+    if (!ok && !b->spare.empty()) {
+      PDLP_CUDA(cudaStreamSynchronize(st));
+      for (auto& a : b->spare) cudaFree(a.first);
+      b->spare.clear();
+      b->bytes_spare = 0;
+      if ((frc = fits(&ok))) return frc;
+    }
+    if (!ok) return fail(PDLP_ERR_OOM, "admission refused: the LP does not fit the memory budget");
+    e = cudaMalloc(&arena, L.total);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(PDLP_ERR_OOM, std::string("admission refused: cudaMalloc: ") + cudaGetErrorString(e));
+    }
   }
   char* base = (char*)arena;
   auto at = [&](size_t off) { return (void*)(base + off); };
   int rc = PDLP_OK;
-  auto cleanup = [&](int code) { cudaStreamSynchronize(st); cudaFree(arena); return code; };
+  auto give_back = [&]() {      // a refused LP's arena returns to the spares
+    b->spare.push_back({arena, arena_bytes});
+    b->bytes_spare += arena_bytes;
+  };
+  auto cleanup = [&](int code) { cudaStreamSynchronize(st); give_back(); return code; };
 
   const int mem = P->memory;
   // pointers: copy int64 into scratch, convert to int32 with checks
@@ -715,9 +758,9 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
   int herr = 0;
   PDLP_CUDA(cudaMemcpyAsync(&herr, err_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
   e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) { cudaFree(arena); return cuda_fail(e, "admission copies"); }
-  if (herr & 1) { cudaFree(arena); return fail(PDLP_ERR_ARG, "malformed sparse structure (pointer or index out of range)"); }
-  if (herr & 2) { cudaFree(arena); return fail(PDLP_ERR_NUMERICAL, "NaN in the data, or an infinite matrix entry or cost"); }
+  if (e != cudaSuccess) { give_back(); return cuda_fail(e, "admission copies"); }
+  if (herr & 1) { give_back(); return fail(PDLP_ERR_ARG, "malformed sparse structure (pointer or index out of range)"); }
+  if (herr & 2) { give_back(); return fail(PDLP_ERR_NUMERICAL, "NaN in the data, or an infinite matrix entry or cost"); }
 
   Slot& S = b->slots[slot];
   S = Slot();
@@ -725,7 +768,7 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
   S.running = true;
   S.m = m; S.n = n; S.nnz = nnz;
   S.arena = arena;
-  S.bytes = L.total;
+  S.bytes = arena_bytes;
   Inst& I = S.inst;
   std::memset(&I, 0, sizeof(I));
   I.m = m; I.n = n; I.nnz = nnz;
@@ -782,7 +825,7 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
   PDLP_CUDA(cudaMemcpyAsync(&b->d_state[slot], &init, sizeof(State), cudaMemcpyHostToDevice, st));
   PDLP_CUDA(cudaMemsetAsync(b->d_counters + 2 * slot, 0, 2 * sizeof(unsigned), st));
   PDLP_CUDA(cudaStreamSynchronize(st));
-  b->bytes_held += L.total;
+  b->bytes_held += arena_bytes;
   b->n_running += 1;
   b->iters_before[slot] = 0;
   b->dirty = true;
@@ -988,7 +1031,8 @@ int pdlp_batch_retire(pdlp_batch* b, int32_t slot) {
   Slot& s = b->slots[slot];
   PDLP_CUDA(cudaStreamSynchronize(b->stream));
   if (s.running) { b->n_running -= 1; }
-  cudaFree(s.arena);
+  b->spare.push_back({s.arena, s.bytes});
+  b->bytes_spare += s.bytes;
   b->bytes_held -= s.bytes;
   s = Slot();
   b->dirty = true;

@@ -16,7 +16,7 @@ namespace pdlp {
 
 constexpr int kWarps = 4;              // warps per block (engine kernels)
 constexpr int kBlock = 32 * kWarps;    // threads per block
-constexpr int kWTileRows = 128;        // rows per normal tile
+constexpr int kWTileRows = 64;         // rows per normal tile
 constexpr int kWTileNnz = 512;         // entries per normal tile
 constexpr int kVecs = 7;               // vectors staged for a hot-mode epilogue
 constexpr double kRuizTol = 1e-2;      // scaling.py:149

@@ -123,6 +123,33 @@ __device__ __forceinline__ const Inst& warp_inst(const EngineArgs& A, int inst, 
   return W.inst;
 }
 
+// The scheduling fields of one LP's state as one warp saw them in the current
+// pass.  They cannot change while a tile of that LP is still unprocessed in
+// the pass: only the LP's finisher writes them, and it runs after the LP's
+// last tile of the pass has completed.  So a warp reads them once per LP per
+// pass instead of once per tile (a cache is declared per pass and starts
+// empty).
+struct PassCache {
+  int inst = -1;
+  int mode = 0, aux = 0, commit = 0;
+  double eta = 0.0, omega = 0.0;
+  __device__ void load_r(const State* S, int id) {
+    inst = id;
+    mode = ld_mut(&S->rmode);
+    commit = ld_mut(&S->ycommit);
+    eta = ld_mut(&S->eta);
+    omega = ld_mut(&S->omega);
+  }
+  __device__ void load_c(const State* S, int id) {
+    inst = id;
+    mode = ld_mut(&S->cmode);
+    aux = ld_mut(&S->cprimal);
+    commit = ld_mut(&S->xcommit);
+    eta = ld_mut(&S->eta);
+    omega = ld_mut(&S->omega);
+  }
+};
+
 // ---- A pass ---------------------------------------------------------------
 
 __device__ void r_finish(const EngineArgs& A, const Inst& I, State* S, int rmode, const double* red) {
@@ -194,7 +221,7 @@ __device__ __forceinline__ void gather_products(const Tile& t, const double* src
 #pragma unroll
   for (int u = 0; u < kWTileNnz / 32; ++u) {
     const int q = lane + 32 * u;
-    g[u] = q < cnt ? ld_mut(src + idx[q]) : 0.0;
+    g[u] = q < cnt ? ld_gather(src + idx[q]) : 0.0;
   }
 #pragma unroll
   for (int u = 0; u < kWTileNnz / 32; ++u) {
@@ -213,7 +240,7 @@ __device__ __forceinline__ void gather_products_f32(const Tile& t, const float* 
 #pragma unroll
   for (int u = 0; u < kWTileNnz / 32; ++u) {
     const int q = lane + 32 * u;
-    g[u] = q < cnt ? __ldcg(src + idx[q]) : 0.0f;
+    g[u] = q < cnt ? ld_gather(src + idx[q]) : 0.0f;
   }
 #pragma unroll
   for (int u = 0; u < kWTileNnz / 32; ++u) {
@@ -405,7 +432,8 @@ __device__ void hot_ctile(const EngineArgs& A, const Tile& t, int ti, const Inst
   }
 }
 
-__device__ void process_rtile(const EngineArgs& A, const Tile t, int ti, WarpSmem& W, int lane) {
+__device__ void process_rtile(const EngineArgs& A, const Tile t, int ti, WarpSmem& W, int lane,
+                              PassCache& pc) {
 #ifdef PDLP_TRACE
   if (A.trace && blockIdx.x == 0 && threadIdx.x == 0) {
     const long long k = A.trace[1279];
@@ -425,9 +453,10 @@ __device__ void process_rtile(const EngineArgs& A, const Tile t, int ti, WarpSme
                  : stage<8>(W.sval, I.rx, t.p0, t.cnt, lane);
   }
   cp_async_commit();
-  const int rmode = ld_mut(&S->rmode);
-  const bool commit = ld_mut(&S->ycommit) != 0;
-  const double eta = ld_mut(&S->eta), omega = ld_mut(&S->omega);
+  if (pc.inst != t.inst) pc.load_r(S, t.inst);
+  const int rmode = pc.mode;
+  const bool commit = pc.commit != 0;
+  const double eta = pc.eta, omega = pc.omega;
   if (rmode == R_NONE) {
     cp_async_wait<0>();
     __syncwarp();
@@ -899,7 +928,8 @@ __device__ void c_finish(const EngineArgs& A, const Inst& I, State* S, int cmode
   }
 }
 
-__device__ void process_ctile(const EngineArgs& A, const Tile t, int ti, WarpSmem& W, int lane) {
+__device__ void process_ctile(const EngineArgs& A, const Tile t, int ti, WarpSmem& W, int lane,
+                              PassCache& pc) {
   State* S = A.st + t.inst;
   const Inst& I = warp_inst(A, t.inst, W, lane);
   int offp = 0, offi = 0, offv = 0;
@@ -910,10 +940,11 @@ __device__ void process_ctile(const EngineArgs& A, const Tile t, int ti, WarpSme
                  : stage<8>(W.sval, I.cx, t.p0, t.cnt, lane);
   }
   cp_async_commit();
-  const int cmode = ld_mut(&S->cmode);
-  const int cprimal = ld_mut(&S->cprimal);
-  const bool xcommit = ld_mut(&S->xcommit) != 0;
-  const double eta = ld_mut(&S->eta), omega = ld_mut(&S->omega);
+  if (pc.inst != t.inst) pc.load_c(S, t.inst);
+  const int cmode = pc.mode;
+  const int cprimal = pc.aux;
+  const bool xcommit = pc.commit != 0;
+  const double eta = pc.eta, omega = pc.omega;
   if (cmode == C_NONE) {
     cp_async_wait<0>();
     __syncwarp();

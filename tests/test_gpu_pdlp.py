@@ -176,3 +176,34 @@ def test_persistent_and_per_pass_launch_agree(require_gpu):
         b = e2.solve_all([prob], params)[0]
     assert a.iterations == b.iterations
     assert np.array_equal(a.x, b.x)
+
+
+def test_retired_arenas_are_reused_and_budget_holds(require_gpu):
+    """A retired slot's device memory serves the next admission: results are
+    bitwise those of a fresh batch, and the memory budget counts the kept
+    arenas (one LP fits the budget, a second does not until the first is
+    retired)."""
+    from sovereign_moe_b200 import _lib
+    from sovereign_moe_b200.batch import BatchEngine
+    small, _ = gc.load("small_known_s0")
+    other, _ = gc.load("small_known_s1")
+    params = PDLPParams(device="gpu", eps_abs=1e-6, eps_rel=1e-6)
+    with BatchEngine(max_slots=1) as eng:
+        fresh = eng.solve_all([small], params)[0]
+    with BatchEngine(max_slots=2) as eng:
+        first = eng.solve_all([other], params)[0]
+        again = eng.solve_all([small], params)[0]     # reuses the retired arena
+        assert np.array_equal(again.x, fresh.x) and again.iterations == fresh.iterations
+        assert first.status == Status.OPTIMAL
+    with BatchEngine(max_slots=2) as probe:
+        need = probe.slot_bytes(small.A.m, small.A.n, small.A.nnz)
+    with BatchEngine(max_slots=2, memory_budget=int(need * 1.5)) as eng:
+        s0 = eng.admit(small, params)
+        with pytest.raises(_lib.PDLPError) as exc:
+            eng.admit(small, params)
+        assert exc.value.code == _lib.PDLP_ERR_OOM
+        eng.run()
+        eng.retire(s0)
+        s1 = eng.admit(small, params)                  # fits again: the arena is reused
+        eng.run()
+        assert np.array_equal(eng.fetch(s1).x, fresh.x)

@@ -45,6 +45,11 @@ WORKLOAD = "uneven_batch_256"
 METRIC = "LP solves/s at rel KKT 1e-6"
 N_LP = 256
 EPS = 1e-6
+# DRAM bytes per algorithmic byte of engine_persistent on this batch, from one
+# ncu capture of the second 256-step launch of
+# `bench.py --workload engine-steps --iters 512`: dram__bytes_read.sum +
+# dram__bytes_write.sum = 93.90 GB against 87.55 GB of algorithmic bytes.
+TRAFFIC_PER_ALGORITHMIC_BYTE = 93.90 / 87.55
 
 
 def load_peaks():
@@ -266,6 +271,7 @@ class GpuArm:
         self.engine_ms = 0.0
         self.engine_bytes = 0.0
         self.engine_launches = 0
+        self.engine_kernels = 0
 
     def step(self, host=False):
         ct, L, c = self.ctypes, self._lib, self.lib
@@ -280,7 +286,9 @@ class GpuArm:
             slots.append(s.value)
         active = ct.c_int32(1)
         while active.value > 0:
+            k0 = c.pdlp_launch_count()
             L.check(c.pdlp_batch_step(self.eng.h, 1 << 16, ct.byref(active)))
+            self.engine_kernels += c.pdlp_launch_count() - k0
             ms, by, _ = self.eng.last_timing()
             self.engine_ms += ms
             self.engine_bytes += by
@@ -348,6 +356,7 @@ def run_gpu(args, rank, world):
     clocks.start()
     arm.engine_ms = arm.engine_bytes = 0.0
     arm.engine_launches = 0
+    arm.engine_kernels = 0
     n0 = lib.pdlp_launch_count()
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -362,6 +371,7 @@ def run_gpu(args, rank, world):
     step_ms = max_over_ranks(dev_ms / args.steps)
     value = N_LP * world / (step_ms / 1000.0)
     eng_ms, eng_bytes, eng_launches = arm.engine_ms, arm.engine_bytes, arm.engine_launches
+    eng_kernels = arm.engine_kernels
 
     # end to end through the C ABI from pinned host buffers (one untimed pass
     # first, so both arms are timed warm)
@@ -403,9 +413,14 @@ def run_gpu(args, rank, world):
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak,
+                         "traffic": (TRAFFIC_PER_ALGORITHMIC_BYTE * eng_bytes / eng_kernels
+                                     if eng_kernels else None),
+                         "traffic_unit": "bytes per launch (ncu ratio x algorithmic bytes)",
+                         "algorithmic_bytes_per_launch": (eng_bytes / eng_kernels
+                                                          if eng_kernels else None),
                          "kernel": "engine_persistent", "peak_source": peak_kind,
-                         "launches": eng_launches, "kernel_ms_per_step": eng_ms / args.steps},
+                         "launches": eng_kernels, "kernel_ms_per_step": eng_ms / args.steps},
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": int(launches),
@@ -513,6 +528,96 @@ def run_engine_steps(args):
     return 0
 
 
+def run_spmv(args):
+    """The standalone CSR SpMV kernel (``pdlp_spmv_f64`` / ``_f32``, the
+    reference Backend's ``spmv``) on the large single-LP matrices: the
+    blending plan (200k x 600k, 3M nnz) and the power-law LP (1M x 3M, 10M
+    nnz at --scale 1), y = A x and y = A^T x.  L2 is flushed (a 256 MB write)
+    before every timed call; each call is timed alone with CUDA events."""
+    import torch
+    from sovereign_moe_b200 import _lib
+    from sovereign_moe_b200.workloads import blending_plan, power_law
+    lib = _lib.load()
+    peak, kind = load_peaks()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    mats = [("blending_plan_200k_x_600k", blending_plan(seed=0).problem)]
+    sc = args.scale
+    mats.append((f"power_law_{int(1e6 * sc)}x{int(3e6 * sc)}",
+                 power_law(seed=0, m=int(1_000_000 * sc), n=int(3_000_000 * sc),
+                           nnz=int(10_000_000 * sc)).problem))
+    rows = []
+    for name, prob in mats:
+        A = prob.A
+        for side, (ptr, idx, val, r, c) in (("A x", (A.rp, A.ri, A.rx, A.m, A.n)),
+                                            ("A^T y", (A.cp, A.ci, A.cx, A.n, A.m))):
+            for prec in ("fp64", "fp32"):
+                dt = torch.float64 if prec == "fp64" else torch.float32
+                es = 8 if prec == "fp64" else 4
+                fn = lib.pdlp_spmv_f64 if prec == "fp64" else lib.pdlp_spmv_f32
+                rp = torch.as_tensor(np.asarray(ptr, np.int64), device="cuda")
+                ri = torch.as_tensor(np.asarray(idx, np.int32), device="cuda")
+                rx = torch.as_tensor(np.asarray(val), device="cuda").to(dt)
+                x = torch.randn(c, dtype=torch.float64, device="cuda").to(dt)
+                y = torch.empty(r, dtype=dt, device="cuda")
+                call = lambda: _lib.check(fn(int(r), rp.data_ptr(), ri.data_ptr(),  # noqa: E731
+                                             rx.data_ptr(), x.data_ptr(), y.data_ptr(),
+                                             stream.cuda_stream))
+                for _ in range(3):
+                    call()
+                times = []
+                for _ in range(args.steps * 10):
+                    flush.zero_()
+                    e0, e1 = _sync_events(torch)
+                    e0.record()
+                    call()
+                    e1.record()
+                    e1.synchronize()
+                    times.append(e0.elapsed_time(e1))
+                nnz = int(idx.shape[0])
+                algo = (es + 4) * nnz + 8 * (r + 1) + es * c + es * r
+                ms = statistics.median(times)
+                rows.append({"matrix": name, "product": side, "dtype": prec, "rows": int(r),
+                             "nnz": nnz, "ms": ms, "algorithmic_bytes": algo,
+                             "GBps": algo / ms / 1e6, "frac_of_measured_hbm": algo / ms / 1e6 / peak})
+                del rp, ri, rx, x, y
+    print(json.dumps({"metric": "SpMV HBM GB/s", "unit": "GB/s", "results": rows,
+                      "peak_GBps": peak, "peak_source": kind,
+                      "l2": "flushed before every call (256 MB write)"}), flush=True)
+    return 0
+
+
+def run_precision(args):
+    """FP32-SpMV against float64 per instance: config-1-shaped known-optimum
+    LPs (230 x 2025, seeds 0-7) and 8 LPs of the uneven batch, each solved at
+    rel KKT 1e-6 in both modes; objective error against the known optimum and
+    between the modes, iterations of each."""
+    from sovereign_moe_b200.batch import BatchEngine
+    from sovereign_moe_b200.pdlp import PDLPParams
+    from sovereign_moe_b200.workloads import single_small, uneven_batch
+    cases = [(f"single_small_s{s}", single_small(seed=s)) for s in range(8)]
+    cases += [(k.problem.name, k) for k in uneven_batch(seed=1000, count=8)]
+    rows = []
+    for name, k in cases:
+        out = {}
+        for prec in ("fp64", "fp32"):
+            p = PDLPParams(device="gpu", eps_abs=EPS, eps_rel=EPS, precision=prec)
+            with BatchEngine(max_slots=1) as eng:
+                out[prec] = eng.solve_all([k.problem], p)[0]
+        f = float(k.f_star)
+        scale = max(1.0, abs(f))
+        rows.append({"lp": name, "rows": int(k.problem.A.m), "cols": int(k.problem.A.n),
+                     "status": [int(out["fp64"].status), int(out["fp32"].status)],
+                     "iterations": [int(out["fp64"].iterations), int(out["fp32"].iterations)],
+                     "rel_err_fp64": abs(out["fp64"].objective - f) / scale,
+                     "rel_err_fp32": abs(out["fp32"].objective - f) / scale,
+                     "rel_diff_fp32_fp64": abs(out["fp32"].objective - out["fp64"].objective) / scale,
+                     "max_abs_dx": float(np.max(np.abs(out["fp32"].x - out["fp64"].x)))})
+    print(json.dumps({"metric": "FP32-SpMV vs FP64 per instance", "tolerance": "rel KKT 1e-6",
+                      "results": rows}), flush=True)
+    return 0
+
+
 def run_serving(args):
     """Poisson arrivals served with continuous batching vs one at a time."""
     from sovereign_moe_b200.serving import Server, latency_summary, serve_one_at_a_time
@@ -545,7 +650,8 @@ def main():
                     help="seconds of CPU work per timed CPU sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="batch",
-                    choices=["batch", "blend", "powerlaw", "serving", "engine-steps"],
+                    choices=["batch", "blend", "powerlaw", "serving", "engine-steps", "spmv",
+                             "precision"],
                     help="batch: the headline metric; the others print auxiliary lines")
     ap.add_argument("--iters", type=int, default=2000)
     ap.add_argument("--scale", type=float, default=1.0)
@@ -563,6 +669,10 @@ def main():
         return run_serving(args)
     if args.workload == "engine-steps":
         return run_engine_steps(args)
+    if args.workload == "spmv":
+        return run_spmv(args)
+    if args.workload == "precision":
+        return run_precision(args)
     if args.warmup < 3 and args.impl == "ours":
         ap.error("--warmup must be >= 3")
     rank = int(os.environ.get("RANK", "0"))

@@ -174,3 +174,36 @@ def verify(prob, x, claimed_obj=None, feas_tol=1e-6, int_tol=1e-6, y=None, opt_t
                     v.add("optimality", rel <= opt_tol,
                           f"certified bound {bound:.12g}, gap {gap:.3e} ({rel:.2e} relative)")
     return v
+
+
+def verify_files(prob, solution_path, feas_tol=1e-6, int_tol=1e-6):
+    """bench/verify.py:279-318 without the MPS read: the solution file is a
+    JSON payload with ``x`` (list or name-keyed object), optional ``objective``
+    and optional ``y`` (list or name-keyed object), or a bare list of x."""
+    import json
+    with open(solution_path, encoding="utf-8") as fh:
+        data = json.load(fh)
+    y = None
+    if isinstance(data, dict) and "x" in data:
+        if isinstance(data["x"], dict):
+            names = {nm: i for i, nm in enumerate(prob.col_names or [])}
+            x = np.zeros(prob.A.n)
+            for nm, val in data["x"].items():
+                if nm in names:
+                    x[names[nm]] = val
+        else:
+            x = np.asarray(data["x"], dtype=float)
+        claimed = data.get("objective")
+        if data.get("y") is not None:
+            if isinstance(data["y"], dict):
+                rnames = {nm: i for i, nm in enumerate(prob.row_names or [])}
+                y = np.zeros(prob.A.m)
+                for nm, val in data["y"].items():
+                    if nm in rnames:
+                        y[rnames[nm]] = val
+            else:
+                y = np.asarray(data["y"], dtype=float)
+    else:
+        x = np.asarray(data, dtype=float)
+        claimed = None
+    return verify(prob, x, claimed, feas_tol, int_tol, y=y)

@@ -59,8 +59,14 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
   int& flag = *reinterpret_cast<int*>(g_smem + sizeof(WarpSmem) * kWarps);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   WarpSmem& W = ws[warp];
-  if (lane == 0) W.inst_id = -1;
+  if (lane == 0) {
+    W.inst_id = -1;
+    mbar_init(&W.bar[0]);
+    mbar_init(&W.bar[1]);
+    mbar_init_fence();
+  }
   __syncwarp();
+  BulkPhase ph;
   const unsigned nb = gridDim.x;
   const int gw = blockIdx.x * kWarps + warp;
   const int r0 = A.rwarp[gw], r1 = A.rwarp[gw + 1];
@@ -90,7 +96,7 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
       for (int t = r0; t < r1; ++t) {
         const Tile cur = next;
         if (t + 1 < r1) next = A.rtiles[t + 1];      // prefetch the next descriptor
-        process_rtile(A, cur, t, W, lane, pc);
+        process_rtile(A, cur, t, W, lane, pc, ph);
       }
     }
     PDLP_STAMP(step, 1);
@@ -103,7 +109,7 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
       for (int t = c0; t < c1; ++t) {
         const Tile cur = next;
         if (t + 1 < c1) next = A.ctiles[t + 1];
-        process_ctile(A, cur, t, W, lane, pc);
+        process_ctile(A, cur, t, W, lane, pc, ph);
       }
     }
     PDLP_STAMP(step, 3);
@@ -119,15 +125,21 @@ __global__ void __launch_bounds__(kBlock, 3) engine_pass(EngineArgs A, int side)
   WarpSmem* ws = reinterpret_cast<WarpSmem*>(g_smem);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   WarpSmem& W = ws[warp];
-  if (lane == 0) W.inst_id = -1;
+  if (lane == 0) {
+    W.inst_id = -1;
+    mbar_init(&W.bar[0]);
+    mbar_init(&W.bar[1]);
+    mbar_init_fence();
+  }
   __syncwarp();
   const int gw = blockIdx.x * kWarps + warp;
   const int nw = gridDim.x * kWarps;
   PassCache pc;
+  BulkPhase ph;
   if (side == 0) {
-    for (int t = gw; t < A.n_rtiles; t += nw) process_rtile(A, A.rtiles[t], t, W, lane, pc);
+    for (int t = gw; t < A.n_rtiles; t += nw) process_rtile(A, A.rtiles[t], t, W, lane, pc, ph);
   } else {
-    for (int t = gw; t < A.n_ctiles; t += nw) process_ctile(A, A.ctiles[t], t, W, lane, pc);
+    for (int t = gw; t < A.n_ctiles; t += nw) process_ctile(A, A.ctiles[t], t, W, lane, pc, ph);
   }
 }
 
@@ -300,6 +312,12 @@ struct pdlp_batch {
   State* h_state = nullptr;
   int sms = 0, coop_blocks_per_sm = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // per-pass mode: `graph_chunk` steps (two launches each) captured once per
+  // tile-list rebuild on a private stream and replayed on the batch's stream
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int64_t graph_chunk = 0;
+  bool graph_stale = true;
   double last_ms = 0.0, last_bytes = 0.0;
   long long last_iters = 0;
   std::vector<long long> iters_before;
@@ -492,6 +510,7 @@ static int rebuild(pdlp_batch* b) {
   // the staging vectors die at return: wait for the copies
   PDLP_CUDA(cudaStreamSynchronize(st));
   b->dirty = false;
+  b->graph_stale = true;
   return PDLP_OK;
 }
 
@@ -592,6 +611,9 @@ int pdlp_batch_create(const pdlp_batch_config* cfg, void* stream, pdlp_batch** o
   cudaMemcpyAsync(b->d_inst, zero.data(), sizeof(Inst) * zero.size(), cudaMemcpyHostToDevice, b->stream);
   cudaEventCreate(&b->ev0);
   cudaEventCreate(&b->ev1);
+  if (!b->cfg.persistent &&
+      (e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return bail(e, "cudaStreamCreateWithFlags");
   if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return bail(e, "cudaStreamSynchronize");
   *out = b;
   return PDLP_OK;
@@ -606,6 +628,8 @@ int pdlp_batch_destroy(pdlp_batch* b) {
   cudaFree(b->d_rtiles); cudaFree(b->d_ctiles); cudaFree(b->d_rwarp); cudaFree(b->d_cwarp);
   cudaFree(b->d_partials); cudaFree(b->d_group_tiles); cudaFree(b->d_gpartials);
   cudaFree(b->d_gcounters);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
   if (b->h_ctl) cudaFreeHost(b->h_ctl);
   if (b->h_state) cudaFreeHost(b->h_state);
   if (b->ev0) cudaEventDestroy(b->ev0);
@@ -809,7 +833,7 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
   I.theta = prm.primal_weight_smoothing;
   plan_tiles(rp, m, slot, b->cfg.tile_rows, b->cfg.tile_nnz, S.rt, S.rtw);
   plan_tiles(cp, n, slot, b->cfg.tile_rows, b->cfg.tile_nnz, S.ct, S.ctw);
-  // algorithmic bytes of one PDHG iteration (see DESIGN.md): value + index per
+  // algorithmic bytes of one PDHG iteration: value + index per
   // entry and pointer per row on both passes, one gathered word per column /
   // row, the vectors each pass reads and writes
   S.bytes_per_iter = f32 ? 16.0 * (double)nnz + 4.0 * (m + 1) + 4.0 * (n + 1) +
@@ -877,15 +901,30 @@ int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out) {
                                             args, kSmemBytes, st));
       count_launches(1);
     } else {
-      const int cap = b->sms * b->coop_blocks_per_sm;
-      const int g_r = std::max(1, std::min((b->n_rtiles + kWarps - 1) / kWarps, cap));
-      const int g_c = std::max(1, std::min((b->n_ctiles + kWarps - 1) / kWarps, cap));
-      for (int64_t s = 0; s < chunk; ++s) {
-        engine_pass<<<g_r, kBlock, kSmemBytes, st>>>(A, 0);
-        engine_pass<<<g_c, kBlock, kSmemBytes, st>>>(A, 1);
+      if (b->graph_stale || !b->graph || b->graph_chunk != chunk) {
+        if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+        const int cap = b->sms * b->coop_blocks_per_sm;
+        const int g_r = std::max(1, std::min((b->n_rtiles + kWarps - 1) / kWarps, cap));
+        const int g_c = std::max(1, std::min((b->n_ctiles + kWarps - 1) / kWarps, cap));
+        cudaStream_t cs = b->cap_stream;
+        PDLP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        for (int64_t s2 = 0; s2 < chunk; ++s2) {
+          engine_pass<<<g_r, kBlock, kSmemBytes, cs>>>(A, 0);
+          engine_pass<<<g_c, kBlock, kSmemBytes, cs>>>(A, 1);
+        }
+        cudaGraph_t g = nullptr;
+        const cudaError_t le = cudaGetLastError();
+        const cudaError_t ce = cudaStreamEndCapture(cs, &g);
+        if (le != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(le, "engine_pass capture"); }
+        if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+        const cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) { b->graph = nullptr; return cuda_fail(ie, "cudaGraphInstantiate"); }
+        b->graph_chunk = chunk;
+        b->graph_stale = false;
       }
+      PDLP_CUDA(cudaGraphLaunch(b->graph, st));
       count_launches(2 * chunk);
-      PDLP_CUDA(cudaGetLastError());
     }
     PDLP_CUDA(cudaEventRecord(b->ev1, st));
     PDLP_CUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, st));

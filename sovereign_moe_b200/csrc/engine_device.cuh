@@ -22,11 +22,13 @@ constexpr int kVecs = 7;               // vectors staged for a hot-mode epilogue
 constexpr double kRuizTol = 1e-2;      // scaling.py:149
 constexpr unsigned kFull = 0xffffffffu;
 
-// Per-warp shared memory.  The s* arrays receive 16-byte asynchronous copies
-// of a tile's row pointers, indices, values and epilogue vectors; each has
-// room for the alignment offset of the copied range.  sval doubles as the
-// products' staging area.
+// Per-warp shared memory.  The s* arrays receive bulk asynchronous copies
+// (whole 16-byte chunks) of a tile's row pointers, indices, values and
+// epilogue vectors; each has room for the alignment offset of the copied
+// range.  sval doubles as the products' staging area.  bar[0] tracks the
+// matrix copies of the current tile, bar[1] its epilogue vectors.
 struct __align__(16) WarpSmem {
+  unsigned long long bar[2];
   int sptr[kWTileRows + 8];
   int sidx[kWTileNnz + 8];
   double sval[kWTileNnz + 4];
@@ -36,6 +38,79 @@ struct __align__(16) WarpSmem {
   int inst_id;
   int pad[3];
   Inst inst;                           // cached descriptor of inst_id
+};
+
+// ---- bulk asynchronous staging (cp.async.bulk + mbarrier) --------------------
+//
+// One lane of a warp arms the warp's mbarrier with the byte count of a group
+// of copies and issues them; the copy engine writes shared memory and
+// completes the barrier's phase when every byte has landed.  Sources are
+// 16-byte aligned (arena arrays start on 256 bytes and ranges are rounded
+// down to a 16-byte chunk); sizes are whole 16-byte chunks, reading at most
+// 15 bytes past a range, which stays inside the slot's arena (every array is
+// followed by padding).
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Orders this warp's earlier shared-memory accesses (generic proxy) before
+// the copy engine's writes (async proxy) into the same buffers.
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+  return ok != 0;
+}
+
+// Whole 16-byte chunks covering elements [first, first + count) of E-byte
+// elements; the copy starts at element first rounded down to a chunk.
+template <int E>
+__device__ __forceinline__ unsigned bulk_bytes(int first, int count) {
+  constexpr int per = 16 / E;
+  if (count <= 0) return 0u;
+  const int a = first & ~(per - 1);
+  return (unsigned)((first + count - a + per - 1) / per) * 16u;
+}
+
+template <int E>
+__device__ __forceinline__ int bulk_offset(int first) {
+  return first & (16 / E - 1);
+}
+
+template <int E>
+__device__ __forceinline__ void bulk_stage(void* dst, const void* base, int first, int count,
+                                           unsigned long long* bar) {
+  const unsigned bytes = bulk_bytes<E>(first, count);
+  if (bytes == 0u) return;
+  const char* src = reinterpret_cast<const char*>(base) + (size_t)(first & ~(16 / E - 1)) * E;
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+
+// Per-warp phase bits of the two barriers, kept in registers for the launch.
+struct BulkPhase {
+  unsigned m = 0, v = 0;
 };
 
 // ---- asynchronous staging (cp.async, 16-byte, L2 only) -----------------------

@@ -250,9 +250,29 @@ __device__ __forceinline__ void gather_products_f32(const Tile& t, const float* 
   __syncwarp();
 }
 
+// Waits for the current phase of one of the warp's copy barriers, then
+// advances the phase bit.  Bounded: after barrier_timeout_ns of wall time it
+// records PDLP_ERR_BARRIER_TIMEOUT (the launch then ends at its next grid
+// barrier) and returns false, and the caller skips the tile's work.
+__device__ bool bulk_wait(const EngineArgs& A, unsigned long long* bar, unsigned& parity) {
+  bool ok = mbar_try_wait(bar, parity);
+  if (!ok) {
+    const long long t0 = global_ns();
+    for (unsigned spins = 1; !ok; ++spins) {
+      ok = mbar_try_wait(bar, parity);
+      if (!ok && (spins & 63u) == 0u && global_ns() - t0 > A.barrier_timeout_ns) {
+        atomicCAS(&A.ctl->error, 0, PDLP_ERR_BARRIER_TIMEOUT);
+        break;
+      }
+    }
+  }
+  parity ^= 1u;
+  return ok;
+}
+
 __device__ void hot_rtile(const EngineArgs& A, const Tile& t, int ti, const Inst& I, State* S,
                           WarpSmem& W, int lane, int rmode, bool commit, double eta,
-                          double omega, int offp, int offi, int offv) {
+                          double omega, int offp, int offi, int offv, BulkPhase& ph) {
 #ifdef PDLP_TRACE
   // stage timestamps of the first warp of block 0 (slots after the step trace)
   // counter in trace[1279], records at trace[640 + 8 k], k < 63
@@ -267,19 +287,23 @@ __device__ void hot_rtile(const EngineArgs& A, const Tile& t, int ti, const Inst
   const int rows = t.end - t.begin;
   const double sigma = eta * omega;
   // vectors: 0 ax, 1 y, 2 rl, 3 ru, 4 sum_y, 5 y_new, 6 adx
-  const int off = stage<8>(W.vec[0], I.ax, t.begin, rows, lane);
-  stage<8>(W.vec[1], I.y, t.begin, rows, lane);
-  stage<8>(W.vec[2], I.rl, t.begin, rows, lane);
-  stage<8>(W.vec[3], I.ru, t.begin, rows, lane);
-  if (rmode == R_ITER || commit) stage<8>(W.vec[4], I.sumy, t.begin, rows, lane);
-  if (commit) {
-    stage<8>(W.vec[5], I.ynew, t.begin, rows, lane);
-    stage<8>(W.vec[6], I.adx, t.begin, rows, lane);
+  const bool with_sum = rmode == R_ITER || commit;
+  if (lane == 0) {
+    const unsigned b = bulk_bytes<8>(t.begin, rows);
+    mbar_arrive_tx(&W.bar[1], b * (4u + (with_sum ? 1u : 0u) + (commit ? 2u : 0u)));
+    bulk_stage<8>(W.vec[0], I.ax, t.begin, rows, &W.bar[1]);
+    bulk_stage<8>(W.vec[1], I.y, t.begin, rows, &W.bar[1]);
+    bulk_stage<8>(W.vec[2], I.rl, t.begin, rows, &W.bar[1]);
+    bulk_stage<8>(W.vec[3], I.ru, t.begin, rows, &W.bar[1]);
+    if (with_sum) bulk_stage<8>(W.vec[4], I.sumy, t.begin, rows, &W.bar[1]);
+    if (commit) {
+      bulk_stage<8>(W.vec[5], I.ynew, t.begin, rows, &W.bar[1]);
+      bulk_stage<8>(W.vec[6], I.adx, t.begin, rows, &W.bar[1]);
+    }
   }
-  cp_async_commit();
+  const int off = bulk_offset<8>(t.begin);
   HOT_STAMP(1);
-  cp_async_wait<1>();
-  __syncwarp();
+  if (!bulk_wait(A, &W.bar[0], ph.m)) { bulk_wait(A, &W.bar[1], ph.v); return; }
   HOT_STAMP(2);
   if (I.f32) {
     gather_products_f32(t, I.dx32, W, offi, offv, lane);
@@ -292,8 +316,7 @@ __device__ void hot_rtile(const EngineArgs& A, const Tile& t, int ti, const Inst
     staged_row_sums(W.sptr + offp, W.sval + offv, rows, I.lanes_r, W.s0, lane);
   }
   HOT_STAMP(4);
-  cp_async_wait<0>();
-  __syncwarp();
+  if (!bulk_wait(A, &W.bar[1], ph.v)) return;
   HOT_STAMP(5);
   double acc[kNP];
 #pragma unroll
@@ -360,22 +383,26 @@ __device__ void hot_rtile(const EngineArgs& A, const Tile& t, int ti, const Inst
 
 __device__ void hot_ctile(const EngineArgs& A, const Tile& t, int ti, const Inst& I, State* S,
                           WarpSmem& W, int lane, int cmode, int cprimal, bool xcommit,
-                          double eta, double omega, int offp, int offi, int offv) {
+                          double eta, double omega, int offp, int offi, int offv,
+                          BulkPhase& ph) {
   const int rows = t.end - t.begin;
   const double tau = eta / omega;
   const bool iter = cmode == C_ITER;
   const bool xc = iter && xcommit;
   // vectors: 0 aty, 1 x (x_new on a commit), 2 c, 3 lo, 4 hi, 5 sum_x
-  const int off = stage<8>(W.vec[0], I.aty, t.begin, rows, lane);
-  stage<8>(W.vec[1], xc ? I.xnew : I.x, t.begin, rows, lane);
-  stage<8>(W.vec[2], I.c, t.begin, rows, lane);
-  stage<8>(W.vec[3], I.lo, t.begin, rows, lane);
-  stage<8>(W.vec[4], I.hi, t.begin, rows, lane);
-  if (iter) stage<8>(W.vec[5], I.sumx, t.begin, rows, lane);
-  cp_async_commit();
-  if (iter) {
-    cp_async_wait<1>();
-    __syncwarp();
+  if (lane == 0) {
+    const unsigned b = bulk_bytes<8>(t.begin, rows);
+    mbar_arrive_tx(&W.bar[1], b * (iter ? 6u : 5u));
+    bulk_stage<8>(W.vec[0], I.aty, t.begin, rows, &W.bar[1]);
+    bulk_stage<8>(W.vec[1], xc ? I.xnew : I.x, t.begin, rows, &W.bar[1]);
+    bulk_stage<8>(W.vec[2], I.c, t.begin, rows, &W.bar[1]);
+    bulk_stage<8>(W.vec[3], I.lo, t.begin, rows, &W.bar[1]);
+    bulk_stage<8>(W.vec[4], I.hi, t.begin, rows, &W.bar[1]);
+    if (iter) bulk_stage<8>(W.vec[5], I.sumx, t.begin, rows, &W.bar[1]);
+  }
+  const int off = bulk_offset<8>(t.begin);
+  if (iter) {     // only the iteration staged the matrix (the primal step needs none)
+    if (!bulk_wait(A, &W.bar[0], ph.m)) { bulk_wait(A, &W.bar[1], ph.v); return; }
     if (I.f32) {
       gather_products_f32(t, I.dy32, W, offi, offv, lane);
       staged_row_sums_f32(W.sptr + offp, reinterpret_cast<const float*>(W.sval) + offv, rows,
@@ -385,8 +412,7 @@ __device__ void hot_ctile(const EngineArgs& A, const Tile& t, int ti, const Inst
       staged_row_sums(W.sptr + offp, W.sval + offv, rows, I.lanes_c, W.s0, lane);
     }
   }
-  cp_async_wait<0>();
-  __syncwarp();
+  if (!bulk_wait(A, &W.bar[1], ph.v)) return;
   double acc[kNP];
 #pragma unroll
   for (int s = 0; s < kNP; ++s) acc[s] = 0.0;
@@ -433,7 +459,7 @@ __device__ void hot_ctile(const EngineArgs& A, const Tile& t, int ti, const Inst
 }
 
 __device__ void process_rtile(const EngineArgs& A, const Tile t, int ti, WarpSmem& W, int lane,
-                              PassCache& pc) {
+                              PassCache& pc, BulkPhase& ph) {
 #ifdef PDLP_TRACE
   if (A.trace && blockIdx.x == 0 && threadIdx.x == 0) {
     const long long k = A.trace[1279];
@@ -442,31 +468,34 @@ __device__ void process_rtile(const EngineArgs& A, const Tile t, int ti, WarpSme
 #endif
   State* S = A.st + t.inst;
   const Inst& I = warp_inst(A, t.inst, W, lane);
-  // The tile's row pointers, indices and values are immutable: their copies
-  // to shared memory start before the state is read, so the state load and
-  // the matrix stream overlap.
-  int offp = 0, offi = 0, offv = 0;
-  if (!t.heavy) {
-    offp = stage<4>(W.sptr, I.rp, t.begin, t.end - t.begin + 1, lane);
-    offi = stage<4>(W.sidx, I.ri, t.p0, t.cnt, lane);
-    offv = I.f32 ? stage<4>(W.sval, I.rx32, t.p0, t.cnt, lane)
-                 : stage<8>(W.sval, I.rx, t.p0, t.cnt, lane);
-  }
-  cp_async_commit();
   if (pc.inst != t.inst) pc.load_r(S, t.inst);
   const int rmode = pc.mode;
   const bool commit = pc.commit != 0;
   const double eta = pc.eta, omega = pc.omega;
-  if (rmode == R_NONE) {
-    cp_async_wait<0>();
-    __syncwarp();
-    return;
+  if (rmode == R_NONE) return;
+  // the tile's row pointers, indices and values, one bulk copy each
+  int offp = 0, offi = 0, offv = 0;
+  if (!t.heavy) {
+    const int rows1 = t.end - t.begin + 1;
+    __syncwarp();                   // every lane is done with the previous tile's buffers
+    if (lane == 0) {
+      fence_proxy_async();
+      const unsigned bv = I.f32 ? bulk_bytes<4>(t.p0, t.cnt) : bulk_bytes<8>(t.p0, t.cnt);
+      mbar_arrive_tx(&W.bar[0], bulk_bytes<4>(t.begin, rows1) + bulk_bytes<4>(t.p0, t.cnt) + bv);
+      bulk_stage<4>(W.sptr, I.rp, t.begin, rows1, &W.bar[0]);
+      bulk_stage<4>(W.sidx, I.ri, t.p0, t.cnt, &W.bar[0]);
+      if (I.f32) bulk_stage<4>(W.sval, I.rx32, t.p0, t.cnt, &W.bar[0]);
+      else bulk_stage<8>(W.sval, I.rx, t.p0, t.cnt, &W.bar[0]);
+    }
+    offp = bulk_offset<4>(t.begin);
+    offi = bulk_offset<4>(t.p0);
+    offv = I.f32 ? bulk_offset<4>(t.p0) : bulk_offset<8>(t.p0);
   }
   if ((rmode == R_ITER || rmode == R_TRIAL) && !t.heavy) {
-    hot_rtile(A, t, ti, I, S, W, lane, rmode, commit, eta, omega, offp, offi, offv);
+    hot_rtile(A, t, ti, I, S, W, lane, rmode, commit, eta, omega, offp, offi, offv, ph);
     return;
   }
-  cp_async_wait<0>();
+  if (!t.heavy && !bulk_wait(A, &W.bar[0], ph.m)) return;
   __syncwarp();
   const int* tptr = W.sptr + offp;
 
@@ -929,32 +958,40 @@ __device__ void c_finish(const EngineArgs& A, const Inst& I, State* S, int cmode
 }
 
 __device__ void process_ctile(const EngineArgs& A, const Tile t, int ti, WarpSmem& W, int lane,
-                              PassCache& pc) {
+                              PassCache& pc, BulkPhase& ph) {
   State* S = A.st + t.inst;
   const Inst& I = warp_inst(A, t.inst, W, lane);
-  int offp = 0, offi = 0, offv = 0;
-  if (!t.heavy) {
-    offp = stage<4>(W.sptr, I.cp, t.begin, t.end - t.begin + 1, lane);
-    offi = stage<4>(W.sidx, I.ci, t.p0, t.cnt, lane);
-    offv = I.f32 ? stage<4>(W.sval, I.cx32, t.p0, t.cnt, lane)
-                 : stage<8>(W.sval, I.cx, t.p0, t.cnt, lane);
-  }
-  cp_async_commit();
   if (pc.inst != t.inst) pc.load_c(S, t.inst);
   const int cmode = pc.mode;
   const int cprimal = pc.aux;
   const bool xcommit = pc.commit != 0;
   const double eta = pc.eta, omega = pc.omega;
-  if (cmode == C_NONE) {
-    cp_async_wait<0>();
-    __syncwarp();
+  if (cmode == C_NONE) return;
+  const bool hot = (cmode == C_ITER || cmode == C_PRIMAL) && !t.heavy;
+  // the tile's column pointers, row indices and values (not needed by the
+  // staged primal step, which reads only vectors)
+  int offp = 0, offi = 0, offv = 0;
+  __syncwarp();                     // every lane is done with the previous tile's buffers
+  if (lane == 0) fence_proxy_async();
+  if (!t.heavy && !(hot && cmode == C_PRIMAL)) {
+    const int rows1 = t.end - t.begin + 1;
+    if (lane == 0) {
+      const unsigned bv = I.f32 ? bulk_bytes<4>(t.p0, t.cnt) : bulk_bytes<8>(t.p0, t.cnt);
+      mbar_arrive_tx(&W.bar[0], bulk_bytes<4>(t.begin, rows1) + bulk_bytes<4>(t.p0, t.cnt) + bv);
+      bulk_stage<4>(W.sptr, I.cp, t.begin, rows1, &W.bar[0]);
+      bulk_stage<4>(W.sidx, I.ci, t.p0, t.cnt, &W.bar[0]);
+      if (I.f32) bulk_stage<4>(W.sval, I.cx32, t.p0, t.cnt, &W.bar[0]);
+      else bulk_stage<8>(W.sval, I.cx, t.p0, t.cnt, &W.bar[0]);
+    }
+    offp = bulk_offset<4>(t.begin);
+    offi = bulk_offset<4>(t.p0);
+    offv = I.f32 ? bulk_offset<4>(t.p0) : bulk_offset<8>(t.p0);
+  }
+  if (hot) {
+    hot_ctile(A, t, ti, I, S, W, lane, cmode, cprimal, xcommit, eta, omega, offp, offi, offv, ph);
     return;
   }
-  if ((cmode == C_ITER || cmode == C_PRIMAL) && !t.heavy) {
-    hot_ctile(A, t, ti, I, S, W, lane, cmode, cprimal, xcommit, eta, omega, offp, offi, offv);
-    return;
-  }
-  cp_async_wait<0>();
+  if (!t.heavy && !bulk_wait(A, &W.bar[0], ph.m)) return;
   __syncwarp();
   const int* tptr = W.sptr + offp;
 

@@ -5,6 +5,8 @@
 #include <cmath>
 #include <mutex>
 #include <string>
+#include <unordered_map>
+#include <utility>
 
 #include "common.cuh"
 
@@ -48,16 +50,35 @@ __global__ void __launch_bounds__(kT) spmv_kernel(int m, const int64_t* __restri
   if (row < m && lane == 0) y[row] = acc;
 }
 
+// Lanes per row of a matrix, remembered by its row-pointer address: the
+// entry point is given no nnz, so the first call on a matrix reads rp[m] back
+// (one synchronisation) and later calls reuse the choice.  A stale entry (a
+// freed and reused address) only changes the lane count, never the result
+// beyond rounding order.
+std::mutex lanes_mu;
+std::unordered_map<const void*, std::pair<int, int>> lanes_cache;   // rp -> (m, L)
+
 template <typename T>
 int launch_spmv(int m, const int64_t* rp, const int* ri, const T* rx, const T* x, T* y,
                 cudaStream_t st) {
   if (m < 0) return fail(PDLP_ERR_ARG, "m must be >= 0");
   if (m == 0) return PDLP_OK;
   if (!rp || !ri || !rx || !x || !y) return fail(PDLP_ERR_ARG, "NULL pointer");
-  int64_t nnz = 0;
-  PDLP_CUDA(cudaMemcpyAsync(&nnz, rp + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  PDLP_CUDA(cudaStreamSynchronize(st));
-  const int L = lanes_of(nnz, m);
+  int L = 0;
+  {
+    std::lock_guard<std::mutex> lock(lanes_mu);
+    auto it = lanes_cache.find(rp);
+    if (it != lanes_cache.end() && it->second.first == m) L = it->second.second;
+  }
+  if (L == 0) {
+    int64_t nnz = 0;
+    PDLP_CUDA(cudaMemcpyAsync(&nnz, rp + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    PDLP_CUDA(cudaStreamSynchronize(st));
+    L = lanes_of(nnz, m);
+    std::lock_guard<std::mutex> lock(lanes_mu);
+    if (lanes_cache.size() >= 256) lanes_cache.clear();
+    lanes_cache[rp] = {m, L};
+  }
   const long long threads = (long long)m * L;
   const int g = grid_1d(threads);
   switch (L) {

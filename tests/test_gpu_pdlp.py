@@ -207,3 +207,25 @@ def test_retired_arenas_are_reused_and_budget_holds(require_gpu):
         s1 = eng.admit(small, params)                  # fits again: the arena is reused
         eng.run()
         assert np.array_equal(eng.fetch(s1).x, fresh.x)
+
+
+def test_cancel_ends_as_interrupted(require_gpu):
+    """A cancelled slot stops at its next check boundary with INTERRUPTED,
+    keeps no objective, and leaves the other slots running to optimality."""
+    from sovereign_moe_b200.batch import BatchEngine
+    a, _ = gc.load("small_known_s0")
+    b, exp_b = gc.load("small_known_s1")
+    params = PDLPParams(device="gpu", eps_abs=1e-12, eps_rel=1e-12, max_iter=100_000)
+    ok = PDLPParams(device="gpu", eps_abs=1e-6, eps_rel=1e-6)
+    with BatchEngine(max_slots=2) as eng:
+        sa = eng.admit(a, params)        # would run to max_iter at 1e-12
+        sb = eng.admit(b, ok)
+        eng.step(200)
+        eng.cancel(sa)
+        eng.run()
+        ra, rb = eng.fetch(sa), eng.fetch(sb)
+    assert ra.status == Status.INTERRUPTED
+    assert np.isnan(ra.objective)
+    assert ra.iterations < 100_000
+    assert rb.status == Status.OPTIMAL
+    assert abs(rb.objective - float(exp_b.known)) / max(1.0, abs(float(exp_b.known))) < 1e-6

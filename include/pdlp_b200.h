@@ -192,7 +192,12 @@ int pdlp_batch_last_timing(pdlp_batch* b, double* ms, double* iter_bytes,
 /* ---- kernel-level Backend (backend.py:317-493) -------------------------- *
  * Device pointers; `stream` as above.  FP64 unless named _f32. */
 
-/* y = A x, A in CSR with int64 pointers (backend.py:373-384) */
+/* y = A x, A in CSR with int64 pointers (backend.py:373-384).  Asynchronous
+ * on `stream`; a fixed summation order, so repeated calls give the same bits.
+ * Rows longer than 256 entries are summed by a second launch from a per-
+ * (device, stream) list that the library keeps between calls.  It is
+ * allocated on the first call with a given stream and grown when a larger m
+ * comes; those calls synchronise the stream. */
 int pdlp_spmv_f64(int32_t m, const int64_t* rp, const int32_t* ri, const double* rx,
                   const double* x, double* y, void* stream);
 int pdlp_spmv_f32(int32_t m, const int64_t* rp, const int32_t* ri, const float* rx,

@@ -4,8 +4,8 @@
 #include <algorithm>
 #include <cmath>
 #include <mutex>
+#include <map>
 #include <string>
-#include <unordered_map>
 #include <utility>
 
 #include "common.cuh"
@@ -21,42 +21,171 @@ int grid_1d(long long n, int per = kT) {
   return (int)std::max(1LL, std::min(g, 1LL << 20));
 }
 
-// Lanes per row from the mean row length (power of two in [1, 32]).
-int lanes_of(long long nnz, long long rows) {
-  if (rows <= 0) return 1;
-  const double avg = (double)nnz / (double)rows;
-  int L = 1;
-  while (L < 32 && L < avg) L <<= 1;
-  return L;
-}
+// y = A x in two launches, with a fixed summation order.
+//
+// spmv_rows32_kernel: one warp per block of 32 consecutive rows.  Rows with
+// more than kLongRow entries are not summed here: the warp appends them to a
+// list (order immaterial) and leaves them to the second launch.  For the
+// others, the warp streams the block's entries in chunks of 128, four per
+// lane and coalesced, with every index, value and gather of a chunk in
+// flight together.  It finds each entry's row by a binary search over the
+// block's row starts, held one per lane.  A segmented shuffle scan sums a
+// row's entries within a 32-entry slice, and the slices are added in order.
+// An entry of a long row inside a chunk is treated as belonging to no row.
+//
+// spmv_long_rows_kernel: one block of 8 warps per listed long row (grid-
+// stride).  Chunk c of the row goes to warp c mod 8, which keeps a per-lane
+// running sum.  A warp tree and then the 8 warp sums in order give the row
+// sum.  So the result of every row is independent of the list order and of
+// the launch shape, and repeated calls give the same bits.
+constexpr int kSpmvWarps = 8;
+constexpr int kLongRow = 256;
 
-// y = A x with L lanes per row: each lane sums its strided entries in order,
-// a xor butterfly combines them (fixed order, so repeats are bitwise equal).
-template <typename T, int L>
-__global__ void __launch_bounds__(kT) spmv_kernel(int m, const int64_t* __restrict__ rp,
-                                                  const int* __restrict__ ri,
-                                                  const T* __restrict__ rx,
-                                                  const T* __restrict__ x, T* __restrict__ y) {
-  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int row = gtid / L;
-  const int lane = threadIdx.x & (L - 1);
-  T acc = T(0);
-  if (row < m) {
-    const int64_t p0 = __ldg(rp + row), p1 = __ldg(rp + row + 1);
-    for (int64_t p = p0 + lane; p < p1; p += L) acc += __ldg(rx + p) * __ldg(x + __ldg(ri + p));
-  }
+constexpr int kSpmvPer = 4;      // entries per lane in one chunk (a chunk is 128 entries)
+
+template <typename T>
+__global__ void __launch_bounds__(kSpmvWarps * 32) spmv_rows32_kernel(
+    int m, const int64_t* __restrict__ rp, const int* __restrict__ ri,
+    const T* __restrict__ rx, const T* __restrict__ x, T* __restrict__ y,
+    int* __restrict__ long_rows) {
+  constexpr int kChunk = 32 * kSpmvPer;
+  __shared__ T acc_s[kSpmvWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  T* acc = acc_s[w];
+  const long long nblk = ((long long)m + 31) / 32;
+  const long long stride = (long long)gridDim.x * kSpmvWarps;
+  for (long long b = (long long)blockIdx.x * kSpmvWarps + w; b < nblk; b += stride) {
+    const int r0 = (int)(b * 32);
+    const int nr = min(32, m - r0);
+    const long long rs = lane < nr ? (long long)__ldg(rp + r0 + lane) : 0LL;
+    const long long re = lane < nr ? (long long)__ldg(rp + r0 + lane + 1) : 0LL;
+    const long long P1 = __shfl_sync(kAll, re, nr - 1);
+    const long long P0 = __shfl_sync(kAll, rs, 0);
+    const bool is_long = lane < nr && re - rs > kLongRow;
+    if (is_long) long_rows[1 + atomicAdd(long_rows, 1)] = r0 + lane;
+    const unsigned long_mask = __ballot_sync(kAll, is_long);
+    acc[lane] = T(0);
+    __syncwarp();
+    // row of entry p: the largest row i < nr with start(i) <= p
+    auto row_of = [&](long long p) {
+      int lo = 0;
 #pragma unroll
-  for (int off = L >> 1; off > 0; off >>= 1) acc += __shfl_xor_sync(kAll, acc, off);
-  if (row < m && lane == 0) y[row] = acc;
+      for (int step = 16; step >= 1; step >>= 1) {
+        const int mid = lo + step;
+        const long long v = __shfl_sync(kAll, rs, mid & 31);
+        if (mid < nr && v <= p) lo = mid;
+      }
+      return lo;
+    };
+    for (long long base = P0; base < P1;) {
+      {                              // a chunk starting in a long row skips to its end
+        const int lo = row_of(base);
+        if ((long_mask >> lo) & 1u) {
+          base = __shfl_sync(kAll, re, lo);
+          continue;
+        }
+      }
+      int row[kSpmvPer], idx[kSpmvPer];
+      T val[kSpmvPer];
+#pragma unroll
+      for (int u = 0; u < kSpmvPer; ++u) {
+        const long long p = base + lane + 32 * u;
+        const int lo = row_of(p);
+        row[u] = (p < P1 && !((long_mask >> lo) & 1u)) ? lo : 32;   // 32: no row
+      }
+#pragma unroll
+      for (int u = 0; u < kSpmvPer; ++u) {
+        const long long p = base + lane + 32 * u;
+        idx[u] = row[u] < 32 ? __ldg(ri + p) : 0;
+        val[u] = row[u] < 32 ? __ldg(rx + p) : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < kSpmvPer; ++u) val[u] = row[u] < 32 ? val[u] * __ldg(x + idx[u]) : T(0);
+#pragma unroll
+      for (int u = 0; u < kSpmvPer; ++u) {
+        T v = val[u];
+        const int r = row[u];
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const T o = __shfl_up_sync(kAll, v, off);
+          const int ro = __shfl_up_sync(kAll, r, off);
+          if (lane >= off && ro == r) v += o;
+        }
+        const int rn = __shfl_down_sync(kAll, r, 1);
+        if (r < 32 && (lane == 31 || rn != r)) acc[r] += v;   // one lane per row
+        __syncwarp();
+      }
+      base += kChunk;
+    }
+    if (lane < nr && !is_long) y[r0 + lane] = acc[lane];
+    __syncwarp();
+  }
 }
 
-// Lanes per row of a matrix, remembered by its row-pointer address: the
-// entry point is given no nnz, so the first call on a matrix reads rp[m] back
-// (one synchronisation) and later calls reuse the choice.  A stale entry (a
-// freed and reused address) only changes the lane count, never the result
-// beyond rounding order.
-std::mutex lanes_mu;
-std::unordered_map<const void*, std::pair<int, int>> lanes_cache;   // rp -> (m, L)
+template <typename T>
+__global__ void __launch_bounds__(kSpmvWarps * 32) spmv_long_rows_kernel(
+    const int64_t* __restrict__ rp, const int* __restrict__ ri, const T* __restrict__ rx,
+    const T* __restrict__ x, T* __restrict__ y, const int* __restrict__ long_rows) {
+  __shared__ T part[kSpmvWarps];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int count = long_rows[0];
+  for (int k = blockIdx.x; k < count; k += gridDim.x) {
+    const int r = long_rows[1 + k];
+    const long long p0 = __ldg(rp + r), p1 = __ldg(rp + r + 1);
+    T sum = T(0);
+    for (long long base = p0 + 128LL * w; base < p1; base += 128LL * kSpmvWarps) {
+      int idx[4];
+      T val[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const long long p = base + lane + 32 * u;
+        idx[u] = p < p1 ? __ldg(ri + p) : 0;
+        val[u] = p < p1 ? __ldg(rx + p) : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const long long p = base + lane + 32 * u;
+        if (p < p1) sum += val[u] * __ldg(x + idx[u]);
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(kAll, sum, off);
+    if (lane == 0) part[w] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      T t = T(0);
+      for (int i = 0; i < kSpmvWarps; ++i) t += part[i];
+      y[r] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// The long-row list (a count, then row indices) of each (device, stream):
+// kept between calls and grown when a larger m comes, so a call allocates
+// nothing in the common case.  Calls on one stream are ordered by the
+// stream; calls on different streams use different lists.
+std::mutex spmv_mu;
+std::map<std::pair<int, cudaStream_t>, std::pair<int*, size_t>> spmv_lists;
+
+int long_row_list(cudaStream_t st, size_t entries, int** out) {
+  int dev = 0;
+  PDLP_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(spmv_mu);
+  auto& slot = spmv_lists[{dev, st}];
+  if (slot.second < entries) {
+    if (slot.first) {
+      PDLP_CUDA(cudaStreamSynchronize(st));
+      cudaFree(slot.first);
+      slot = {nullptr, 0};
+    }
+    const size_t n = std::max(entries, (size_t)1 << 16);
+    PDLP_CUDA(cudaMalloc((void**)&slot.first, sizeof(int) * n));
+    slot.second = n;
+  }
+  *out = slot.first;
+  return PDLP_OK;
+}
 
 template <typename T>
 int launch_spmv(int m, const int64_t* rp, const int* ri, const T* rx, const T* x, T* y,
@@ -64,33 +193,16 @@ int launch_spmv(int m, const int64_t* rp, const int* ri, const T* rx, const T* x
   if (m < 0) return fail(PDLP_ERR_ARG, "m must be >= 0");
   if (m == 0) return PDLP_OK;
   if (!rp || !ri || !rx || !x || !y) return fail(PDLP_ERR_ARG, "NULL pointer");
-  int L = 0;
-  {
-    std::lock_guard<std::mutex> lock(lanes_mu);
-    auto it = lanes_cache.find(rp);
-    if (it != lanes_cache.end() && it->second.first == m) L = it->second.second;
-  }
-  if (L == 0) {
-    int64_t nnz = 0;
-    PDLP_CUDA(cudaMemcpyAsync(&nnz, rp + m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-    PDLP_CUDA(cudaStreamSynchronize(st));
-    L = lanes_of(nnz, m);
-    std::lock_guard<std::mutex> lock(lanes_mu);
-    if (lanes_cache.size() >= 256) lanes_cache.clear();
-    lanes_cache[rp] = {m, L};
-  }
-  const long long threads = (long long)m * L;
-  const int g = grid_1d(threads);
-  switch (L) {
-    case 1: spmv_kernel<T, 1><<<g, kT, 0, st>>>(m, rp, ri, rx, x, y); break;
-    case 2: spmv_kernel<T, 2><<<g, kT, 0, st>>>(m, rp, ri, rx, x, y); break;
-    case 4: spmv_kernel<T, 4><<<g, kT, 0, st>>>(m, rp, ri, rx, x, y); break;
-    case 8: spmv_kernel<T, 8><<<g, kT, 0, st>>>(m, rp, ri, rx, x, y); break;
-    case 16: spmv_kernel<T, 16><<<g, kT, 0, st>>>(m, rp, ri, rx, x, y); break;
-    default: spmv_kernel<T, 32><<<g, kT, 0, st>>>(m, rp, ri, rx, x, y); break;
-  }
+  int* long_rows = nullptr;
+  const int rc = long_row_list(st, (size_t)m + 1, &long_rows);
+  if (rc != PDLP_OK) return rc;
+  PDLP_CUDA(cudaMemsetAsync(long_rows, 0, sizeof(int), st));
+  const long long nblk = ((long long)m + 31) / 32;
+  const int g = (int)std::min((nblk + kSpmvWarps - 1) / kSpmvWarps, 1LL << 30);
+  spmv_rows32_kernel<T><<<g, kSpmvWarps * 32, 0, st>>>(m, rp, ri, rx, x, y, long_rows);
+  spmv_long_rows_kernel<T><<<592, kSpmvWarps * 32, 0, st>>>(rp, ri, rx, x, y, long_rows);
+  count_launches(2);
   PDLP_CUDA(cudaGetLastError());
-  count_launches(1);
   return PDLP_OK;
 }
 

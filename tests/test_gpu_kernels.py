@@ -76,6 +76,29 @@ def test_spmv_handles_empty_and_warp_boundary_rows(bk):
                                rtol=1e-12, atol=1e-12)
 
 
+def test_spmv_long_rows_and_partial_row_blocks(bk):
+    """Rows longer than one 128-entry chunk, empty rows between them, and a
+    last block of fewer than 32 rows, in both value types."""
+    rng = np.random.default_rng(4)
+    lens = rng.choice([0, 1, 5, 31, 32, 33, 127, 128, 129, 300, 1000], size=77)
+    m, n = len(lens), 1500
+    rows = np.repeat(np.arange(m), lens)
+    cols = np.concatenate([rng.choice(n, size=k, replace=False) for k in lens])
+    A = SparseMatrix.from_triplets(rows, cols, rng.standard_normal(rows.size), m, n)
+    x = rng.standard_normal(n)
+    exp = po.spmv(A.rp, A.ri, A.rx, x)
+    out = bk.zeros(m) + 12345.0
+    bk.spmv(*_dev(bk, A), bk.to_device(x), out, m)
+    bk.sync()
+    np.testing.assert_allclose(bk.to_host(out), exp, rtol=1e-12, atol=1e-12)
+    import torch
+    out32 = torch.full((m,), 12345.0, dtype=torch.float32, device="cuda")
+    bk.spmv(bk.pointer(A.rp), bk.index(A.ri), bk.to_device(A.rx).float(),
+            bk.to_device(x).float(), out32, m)
+    bk.sync()
+    np.testing.assert_allclose(out32.cpu().numpy(), exp, rtol=1e-4, atol=1e-3)
+
+
 @pytest.mark.parametrize("k", [1, 8, 32, 33, 64])
 def test_spmm_matches_oracle(bk, k):
     A, rng = _random_csr(300, 500, 4, seed=k)

@@ -26,32 +26,49 @@ int grid_1d(long long n, int per = kT) {
 // spmv_rows32_kernel: one warp per block of 32 consecutive rows.  Rows with
 // more than kLongRow entries are not summed here: the warp appends them to a
 // list (order immaterial) and leaves them to the second launch.  For the
-// others, the warp streams the block's entries in chunks of 128, four per
-// lane and coalesced, with every index, value and gather of a chunk in
-// flight together.  It finds each entry's row by a binary search over the
-// block's row starts, held one per lane.  A segmented shuffle scan sums a
-// row's entries within a 32-entry slice, and the slices are added in order.
-// An entry of a long row inside a chunk is treated as belonging to no row.
+// others the warp picks L lanes per row from the block's own mean row length
+// (a power of two, 1..32), so short rows keep every lane busy without a
+// cross-lane scan.  Each lane sums its strided entries in order, a xor
+// butterfly over the L lanes combines them, and 32/L rows run side by side.
 //
 // spmv_long_rows_kernel: one block of 8 warps per listed long row (grid-
 // stride).  Chunk c of the row goes to warp c mod 8, which keeps a per-lane
 // running sum.  A warp tree and then the 8 warp sums in order give the row
-// sum.  So the result of every row is independent of the list order and of
-// the launch shape, and repeated calls give the same bits.
+// sum.  So the result of every row depends only on the matrix, not on the
+// list order or the launch shape, and repeated calls give the same bits.
 constexpr int kSpmvWarps = 8;
 constexpr int kLongRow = 256;
 
-constexpr int kSpmvPer = 4;      // entries per lane in one chunk (a chunk is 128 entries)
+template <typename T, int L>
+__device__ __forceinline__ void spmv_block_rows(int r0, int nr, long long rs, long long re,
+                                                unsigned long_mask, int lane,
+                                                const int* __restrict__ ri,
+                                                const T* __restrict__ rx,
+                                                const T* __restrict__ x, T* __restrict__ y) {
+  constexpr int G = 32 / L;
+  const int sub = lane & (L - 1), gi = lane / L;
+  for (int g = 0; g < nr; g += G) {
+    const int i = g + gi;                       // row of this lane's group, within the block
+    const long long p0 = __shfl_sync(kAll, rs, i & 31);
+    const long long p1 = __shfl_sync(kAll, re, i & 31);
+    const bool active = i < nr && !((long_mask >> i) & 1u);
+    T acc = T(0);
+    if (active) {
+#pragma unroll 4
+      for (long long p = p0 + sub; p < p1; p += L) acc += __ldg(rx + p) * __ldg(x + __ldg(ri + p));
+    }
+#pragma unroll
+    for (int off = L >> 1; off > 0; off >>= 1) acc += __shfl_xor_sync(kAll, acc, off);
+    if (active && sub == 0) y[r0 + i] = acc;
+  }
+}
 
 template <typename T>
 __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_rows32_kernel(
     int m, const int64_t* __restrict__ rp, const int* __restrict__ ri,
     const T* __restrict__ rx, const T* __restrict__ x, T* __restrict__ y,
     int* __restrict__ long_rows) {
-  constexpr int kChunk = 32 * kSpmvPer;
-  __shared__ T acc_s[kSpmvWarps][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  T* acc = acc_s[w];
   const long long nblk = ((long long)m + 31) / 32;
   const long long stride = (long long)gridDim.x * kSpmvWarps;
   for (long long b = (long long)blockIdx.x * kSpmvWarps + w; b < nblk; b += stride) {
@@ -59,66 +76,21 @@ __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_rows32_kernel(
     const int nr = min(32, m - r0);
     const long long rs = lane < nr ? (long long)__ldg(rp + r0 + lane) : 0LL;
     const long long re = lane < nr ? (long long)__ldg(rp + r0 + lane + 1) : 0LL;
-    const long long P1 = __shfl_sync(kAll, re, nr - 1);
-    const long long P0 = __shfl_sync(kAll, rs, 0);
     const bool is_long = lane < nr && re - rs > kLongRow;
     if (is_long) long_rows[1 + atomicAdd(long_rows, 1)] = r0 + lane;
     const unsigned long_mask = __ballot_sync(kAll, is_long);
-    acc[lane] = T(0);
-    __syncwarp();
-    // row of entry p: the largest row i < nr with start(i) <= p
-    auto row_of = [&](long long p) {
-      int lo = 0;
+    // mean length of the block's short rows -> lanes per row
+    long long len = (lane < nr && !is_long) ? re - rs : 0;
 #pragma unroll
-      for (int step = 16; step >= 1; step >>= 1) {
-        const int mid = lo + step;
-        const long long v = __shfl_sync(kAll, rs, mid & 31);
-        if (mid < nr && v <= p) lo = mid;
-      }
-      return lo;
-    };
-    for (long long base = P0; base < P1;) {
-      {                              // a chunk starting in a long row skips to its end
-        const int lo = row_of(base);
-        if ((long_mask >> lo) & 1u) {
-          base = __shfl_sync(kAll, re, lo);
-          continue;
-        }
-      }
-      int row[kSpmvPer], idx[kSpmvPer];
-      T val[kSpmvPer];
-#pragma unroll
-      for (int u = 0; u < kSpmvPer; ++u) {
-        const long long p = base + lane + 32 * u;
-        const int lo = row_of(p);
-        row[u] = (p < P1 && !((long_mask >> lo) & 1u)) ? lo : 32;   // 32: no row
-      }
-#pragma unroll
-      for (int u = 0; u < kSpmvPer; ++u) {
-        const long long p = base + lane + 32 * u;
-        idx[u] = row[u] < 32 ? __ldg(ri + p) : 0;
-        val[u] = row[u] < 32 ? __ldg(rx + p) : T(0);
-      }
-#pragma unroll
-      for (int u = 0; u < kSpmvPer; ++u) val[u] = row[u] < 32 ? val[u] * __ldg(x + idx[u]) : T(0);
-#pragma unroll
-      for (int u = 0; u < kSpmvPer; ++u) {
-        T v = val[u];
-        const int r = row[u];
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-          const T o = __shfl_up_sync(kAll, v, off);
-          const int ro = __shfl_up_sync(kAll, r, off);
-          if (lane >= off && ro == r) v += o;
-        }
-        const int rn = __shfl_down_sync(kAll, r, 1);
-        if (r < 32 && (lane == 31 || rn != r)) acc[r] += v;   // one lane per row
-        __syncwarp();
-      }
-      base += kChunk;
-    }
-    if (lane < nr && !is_long) y[r0 + lane] = acc[lane];
-    __syncwarp();
+    for (int off = 16; off > 0; off >>= 1) len += __shfl_xor_sync(kAll, len, off);
+    const int shorts = nr - __popc(long_mask);
+    const long long avg = shorts > 0 ? (len + shorts - 1) / shorts : 0;
+    if (avg <= 1) spmv_block_rows<T, 1>(r0, nr, rs, re, long_mask, lane, ri, rx, x, y);
+    else if (avg <= 2) spmv_block_rows<T, 2>(r0, nr, rs, re, long_mask, lane, ri, rx, x, y);
+    else if (avg <= 4) spmv_block_rows<T, 4>(r0, nr, rs, re, long_mask, lane, ri, rx, x, y);
+    else if (avg <= 8) spmv_block_rows<T, 8>(r0, nr, rs, re, long_mask, lane, ri, rx, x, y);
+    else if (avg <= 16) spmv_block_rows<T, 16>(r0, nr, rs, re, long_mask, lane, ri, rx, x, y);
+    else spmv_block_rows<T, 32>(r0, nr, rs, re, long_mask, lane, ri, rx, x, y);
   }
 }
 

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PDLP_ABI_VERSION 1
+#define PDLP_ABI_VERSION 2
 
 /* ---- error codes ------------------------------------------------------- */
 #define PDLP_OK                   0
@@ -45,6 +45,8 @@ extern "C" {
 
 /* ---- statuses: same integers as sovopt Status (src/sovopt/core/problem.py:58-69) */
 #define PDLP_STATUS_OPTIMAL          0
+#define PDLP_STATUS_INFEASIBLE       1
+#define PDLP_STATUS_INFEASIBLE_OR_UNBOUNDED 3
 #define PDLP_STATUS_ITERATION_LIMIT  4
 #define PDLP_STATUS_TIME_LIMIT       5
 #define PDLP_STATUS_NUMERICAL        8
@@ -102,6 +104,16 @@ typedef struct pdlp_params {
                                            (counts against time_limit)       */
     int32_t history_capacity;           /* checks recorded (0 = none)        */
     int32_t precision;                  /* PDLP_PRECISION_*                  */
+    /* Infeasibility detection (no counterpart in the reference, whose PDLP
+     * runs an infeasible LP to its iteration or time limit).  When nonzero,
+     * the change of the iterates between checks of at least 256 iterations is
+     * tested as a Farkas ray: a dual ray certifying primal infeasibility ends
+     * the solve as PDLP_STATUS_INFEASIBLE, and a primal ray certifying dual
+     * infeasibility ends it as PDLP_STATUS_INFEASIBLE_OR_UNBOUNDED; either
+     * must hold at two checks in a row, with a violation at most
+     * eps_infeasible times the ray's objective.  Off by default. */
+    int32_t detect_infeasibility;
+    double eps_infeasible;              /* default 1e-8                      */
 } pdlp_params;
 
 void pdlp_params_default(pdlp_params* p);

@@ -51,7 +51,8 @@ class Params(ctypes.Structure):
                 ("beta_necessary", ctypes.c_double), ("beta_artificial", ctypes.c_double),
                 ("primal_weight_smoothing", ctypes.c_double), ("scaling", ctypes.c_int32),
                 ("power_start", _c_p), ("time_used", ctypes.c_double),
-                ("history_capacity", ctypes.c_int32), ("precision", ctypes.c_int32)]
+                ("history_capacity", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("detect_infeasibility", ctypes.c_int32), ("eps_infeasible", ctypes.c_double)]
 
 
 class Result(ctypes.Structure):

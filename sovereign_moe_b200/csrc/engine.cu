@@ -143,6 +143,126 @@ __global__ void __launch_bounds__(kBlock, 3) engine_pass(EngineArgs A, int side)
   }
 }
 
+// ---- infeasibility certificates (tested between launches) --------------------
+//
+// The candidates are the change of the scaled iterates since the previous
+// test, e = x - x_prev and d = y - y_prev, with both signs s = +1, -1.
+//
+// Dual ray w = s d, with w_i set to 0 where its sign would need an infinite
+// row bound.  For every feasible x, sum_i w_i (Ax)_i >= sum_i q(w_i), where
+// q(w) = w rl if w > 0 and w ru if w < 0.  Also (A^T w)^T x <= sum_j u(g_j),
+// where g = A^T w and u(g) = g hi if g > 0 and g lo if g < 0.  So
+// sum q - sum u > 0 proves the LP infeasible, provided the u terms that would
+// need an infinite bound vanish.  Their largest |g_j| is the violation.
+//
+// Primal ray v = s e, with v_j set to 0 where it would leave a finite column
+// bound.  If c^T v < 0 and A v stays in the recession cone of the row bounds
+// (h_i <= 0 where ru is finite, h_i >= 0 where rl is finite; the largest
+// breach is the violation), the dual is infeasible.
+//
+// Each launch writes 8 partials per block; the host sums them in block order.
+constexpr int kRayBlocks = 592;
+
+__device__ __forceinline__ double ray_w(double d, double rl, double ru) {
+  if (d > 0.0 && rl <= -kInf) return 0.0;
+  if (d < 0.0 && ru >= kInf) return 0.0;
+  return d;
+}
+
+__device__ __forceinline__ double ray_v(double e, double lo, double hi) {
+  if (e > 0.0 && hi < kInf) return 0.0;
+  if (e < 0.0 && lo > -kInf) return 0.0;
+  return e;
+}
+
+// Fixed-order block reduction of 8 values (sums in 0, 1, 4, 5; maxima else).
+__device__ void ray_block_reduce(double (&v)[8], double* out) {
+  __shared__ double sh[8][8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const bool is_sum = k == 0 || k == 1 || k == 4 || k == 5;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double o = __shfl_xor_sync(0xffffffffu, v[k], off);
+      v[k] = is_sum ? v[k] + o : fmax(v[k], o);
+    }
+    if (lane == 0) sh[w][k] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    const int k = threadIdx.x;
+    const bool is_sum = k == 0 || k == 1 || k == 4 || k == 5;
+    double a = sh[0][k];
+    for (int i = 1; i < 8; ++i) a = is_sum ? a + sh[i][k] : fmax(a, sh[i][k]);
+    out[(size_t)blockIdx.x * 8 + k] = a;
+  }
+}
+
+// Columns of A (CSR of A^T): for s = +/-1, sum -u(g_s) (0, 1), violation of
+// g_s (2, 3), sum c_j v_s,j (4, 5) and max |v_s| (6, 7).
+__global__ void __launch_bounds__(256) ray_cols_kernel(Inst I, const double* xprev,
+                                                       const double* yprev, double* part) {
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < I.n; j += gridDim.x * blockDim.x) {
+    double gp = 0.0, gm = 0.0;
+    for (int p = I.cp[j]; p < I.cp[j + 1]; ++p) {
+      const int i = I.ci[p];
+      const double d = I.y[i] - yprev[i];
+      const double a = I.cx[p];
+      gp += a * ray_w(d, I.rl[i], I.ru[i]);
+      gm += a * ray_w(-d, I.rl[i], I.ru[i]);
+    }
+    const double lo = I.lo[j], hi = I.hi[j];
+    const double g2[2] = {gp, gm};
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const double g = g2[s];
+      if (g > 0.0) { if (hi < kInf) v[s] -= g * hi; else v[2 + s] = fmax(v[2 + s], g); }
+      else if (g < 0.0) { if (lo > -kInf) v[s] -= g * lo; else v[2 + s] = fmax(v[2 + s], -g); }
+    }
+    const double e = I.x[j] - xprev[j];
+    const double vp = ray_v(e, lo, hi), vm = ray_v(-e, lo, hi);
+    v[4] += I.c[j] * vp;
+    v[5] += I.c[j] * vm;
+    v[6] = fmax(v[6], fabs(vp));
+    v[7] = fmax(v[7], fabs(vm));
+  }
+  ray_block_reduce(v, part);
+}
+
+// Rows of A (CSR of A): for s = +/-1, sum q(w_s) (0, 1), violation of
+// h_s = A v_s (2, 3), unused (4, 5), max |w_s| (6, 7).
+__global__ void __launch_bounds__(256) ray_rows_kernel(Inst I, const double* xprev,
+                                                       const double* yprev, double* part) {
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < I.m; i += gridDim.x * blockDim.x) {
+    double hp = 0.0, hm = 0.0;
+    for (int p = I.rp[i]; p < I.rp[i + 1]; ++p) {
+      const int j = I.ri[p];
+      const double e = I.x[j] - xprev[j];
+      const double a = I.rx[p];
+      hp += a * ray_v(e, I.lo[j], I.hi[j]);
+      hm += a * ray_v(-e, I.lo[j], I.hi[j]);
+    }
+    const double rl = I.rl[i], ru = I.ru[i];
+    const double h2[2] = {hp, hm};
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const double h = h2[s];
+      if (h > 0.0 && ru < kInf) v[2 + s] = fmax(v[2 + s], h);
+      if (h < 0.0 && rl > -kInf) v[2 + s] = fmax(v[2 + s], -h);
+    }
+    const double d = I.y[i] - yprev[i];
+    const double wp = ray_w(d, rl, ru), wm = ray_w(-d, rl, ru);
+    v[0] += wp > 0.0 ? wp * rl : (wp < 0.0 ? wp * ru : 0.0);
+    v[1] += wm > 0.0 ? wm * rl : (wm < 0.0 ? wm * ru : 0.0);
+    v[6] = fmax(v[6], fabs(wp));
+    v[7] = fmax(v[7], fabs(wm));
+  }
+  ray_block_reduce(v, part);
+}
+
 // ---- admission kernels ----------------------------------------------------------
 
 // All admission checks and the pointer conversions in one launch: task
@@ -266,6 +386,14 @@ void plan_tiles(const int64_t* ptr, int nrows, int inst, int rows_cap, int nnz_c
 struct Slot {
   bool used = false;
   bool running = false;
+  // infeasibility test (between launches): previous iterates, next check
+  bool detect = false;
+  double eps_inf = 1e-8;
+  double* xprev = nullptr;
+  double* yprev = nullptr;
+  bool have_prev = false;
+  long long next_check = 0;
+  int hits = 0, hit_kind = 0;
   int m = 0, n = 0;
   long long nnz = 0;
   void* arena = nullptr;
@@ -314,6 +442,8 @@ struct pdlp_batch {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // per-pass mode: `graph_chunk` steps (two launches each) captured once per
   // tile-list rebuild on a private stream and replayed on the batch's stream
+  double* d_raypart = nullptr;     // infeasibility test partials (2 x kRayBlocks x 8)
+  double* h_raypart = nullptr;
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t graph = nullptr;
   int64_t graph_chunk = 0;
@@ -356,7 +486,7 @@ struct Layout {
 struct SlotLayout {
   size_t rp32, cp32, ri, ci, rx0, cx0, rx, cx, kind, v0, tmp64;
   size_t c0, rl0, ru0, lo0, hi0;
-  size_t mvec[14];   // c-side... see fill
+  size_t mvec[15];   // row-side vectors (the last: previous y of the infeasibility test)
   size_t nvec[16];
   size_t hist;
   size_t rx32, cx32, dx32, dy32;
@@ -382,7 +512,7 @@ SlotLayout layout_for(int m, int n, long long nnz, bool kind, bool v0, int hist_
   s.hi0 = L.take(sizeof(double) * (size_t)n);
   s.rl0 = L.take(sizeof(double) * (size_t)m);
   s.ru0 = L.take(sizeof(double) * (size_t)m);
-  for (int i = 0; i < 14; ++i) s.mvec[i] = L.take(sizeof(double) * (size_t)m);
+  for (int i = 0; i < 15; ++i) s.mvec[i] = L.take(sizeof(double) * (size_t)m);
   for (int i = 0; i < 16; ++i) s.nvec[i] = L.take(sizeof(double) * (size_t)n);
   s.hist = L.take(sizeof(double) * 5 * (size_t)std::max(hist_cap, 0));
   if (f32) {
@@ -514,6 +644,52 @@ static int rebuild(pdlp_batch* b) {
   return PDLP_OK;
 }
 
+// The infeasibility test of one running slot, between launches.  The first
+// call only records the iterates; later calls test the change since the
+// previous call as a Farkas ray and, after two hits of the same kind in a
+// row, return the status to end the solve with in *request (0: none).
+static int infeasibility_test(pdlp_batch* b, Slot& sl, int* request) {
+  *request = 0;
+  const Inst& I = sl.inst;
+  cudaStream_t st = b->stream;
+  const size_t np = sizeof(double) * 8 * kRayBlocks;
+  if (sl.have_prev) {
+    ray_cols_kernel<<<kRayBlocks, 256, 0, st>>>(I, sl.xprev, sl.yprev, b->d_raypart);
+    ray_rows_kernel<<<kRayBlocks, 256, 0, st>>>(I, sl.xprev, sl.yprev, b->d_raypart + 8 * kRayBlocks);
+    count_launches(2);
+    PDLP_CUDA(cudaGetLastError());
+    PDLP_CUDA(cudaMemcpyAsync(b->h_raypart, b->d_raypart, 2 * np, cudaMemcpyDeviceToHost, st));
+  }
+  if (I.n) PDLP_CUDA(cudaMemcpyAsync(sl.xprev, I.x, sizeof(double) * I.n, cudaMemcpyDeviceToDevice, st));
+  if (I.m) PDLP_CUDA(cudaMemcpyAsync(sl.yprev, I.y, sizeof(double) * I.m, cudaMemcpyDeviceToDevice, st));
+  PDLP_CUDA(cudaStreamSynchronize(st));
+  if (!sl.have_prev) { sl.have_prev = true; return PDLP_OK; }
+  double col[8], row[8];
+  for (int side = 0; side < 2; ++side) {
+    double* out = side ? row : col;
+    const double* part = b->h_raypart + (size_t)side * 8 * kRayBlocks;
+    for (int k = 0; k < 8; ++k) {
+      const bool is_sum = k == 0 || k == 1 || k == 4 || k == 5;
+      double a = part[k];
+      for (int g = 1; g < kRayBlocks; ++g) a = is_sum ? a + part[(size_t)g * 8 + k] : std::max(a, part[(size_t)g * 8 + k]);
+      out[k] = a;
+    }
+  }
+  int kind = 0;
+  for (int s = 0; s < 2 && !kind; ++s) {
+    const double dobj = row[s] + col[s], viol = col[2 + s], wmax = row[6 + s];
+    if (wmax > 0.0 && dobj > 0.0 && viol <= sl.eps_inf * dobj) kind = PDLP_STATUS_INFEASIBLE;
+  }
+  for (int s = 0; s < 2 && !kind; ++s) {
+    const double ctv = col[4 + s], viol = row[2 + s], vmax = col[6 + s];
+    if (vmax > 0.0 && ctv < 0.0 && viol <= sl.eps_inf * -ctv) kind = PDLP_STATUS_INFEASIBLE_OR_UNBOUNDED;
+  }
+  if (kind && kind == sl.hit_kind) ++sl.hits;
+  else { sl.hits = kind ? 1 : 0; sl.hit_kind = kind; }
+  if (sl.hits >= 2) *request = kind;
+  return PDLP_OK;
+}
+
 extern "C" {
 
 int pdlp_abi_version(void) { return PDLP_ABI_VERSION; }
@@ -539,6 +715,8 @@ void pdlp_params_default(pdlp_params* p) {
   p->power_start = nullptr;
   p->time_used = 0.0;
   p->history_capacity = 0;
+  p->detect_infeasibility = 0;
+  p->eps_infeasible = 1e-8;
 }
 
 void pdlp_batch_config_default(pdlp_batch_config* c) {
@@ -602,6 +780,10 @@ int pdlp_batch_create(const pdlp_batch_config* cfg, void* stream, pdlp_batch** o
   if ((e = cudaMalloc(&b->d_counters, sizeof(unsigned) * 2 * c.max_slots)) != cudaSuccess) return bail(e, "cudaMalloc");
   if ((e = cudaMalloc(&b->d_ctl, sizeof(Control))) != cudaSuccess) return bail(e, "cudaMalloc");
   if ((e = cudaMallocHost(&b->h_ctl, sizeof(Control))) != cudaSuccess) return bail(e, "cudaMallocHost");
+  if ((e = cudaMalloc(&b->d_raypart, sizeof(double) * 16 * kRayBlocks)) != cudaSuccess)
+    return bail(e, "cudaMalloc");
+  if ((e = cudaMallocHost(&b->h_raypart, sizeof(double) * 16 * kRayBlocks)) != cudaSuccess)
+    return bail(e, "cudaMallocHost");
   if ((e = cudaMallocHost(&b->h_state, sizeof(State) * c.max_slots)) != cudaSuccess) return bail(e, "cudaMallocHost");
   cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2 * c.max_slots, b->stream);
   cudaMemsetAsync(b->d_ctl, 0, sizeof(Control), b->stream);
@@ -628,6 +810,8 @@ int pdlp_batch_destroy(pdlp_batch* b) {
   cudaFree(b->d_rtiles); cudaFree(b->d_ctiles); cudaFree(b->d_rwarp); cudaFree(b->d_cwarp);
   cudaFree(b->d_partials); cudaFree(b->d_group_tiles); cudaFree(b->d_gpartials);
   cudaFree(b->d_gcounters);
+  cudaFree(b->d_raypart);
+  if (b->h_raypart) cudaFreeHost(b->h_raypart);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
   if (b->h_ctl) cudaFreeHost(b->h_ctl);
@@ -816,6 +1000,10 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
   double** nv[16] = {&I.c, &I.lo, &I.hi, &I.cs, &I.x, &I.aty, &I.dx, &I.xnew, &I.sumx,
                      &I.xbar, &I.atybar, &I.atyf, &I.xrst, &I.xout, &I.dout, nullptr};
   for (int i = 0; i < 15; ++i) *nv[i] = (double*)at(L.nvec[i]);
+  S.xprev = (double*)at(L.nvec[15]);
+  S.yprev = (double*)at(L.mvec[14]);
+  S.detect = prm.detect_infeasibility != 0;
+  S.eps_inf = prm.eps_infeasible > 0.0 ? prm.eps_infeasible : 1e-8;
   I.v0 = has_v0 ? (const double*)at(L.v0) : nullptr;
   I.f32 = f32 ? 1 : 0;
   I.rx32 = f32 ? (float*)at(L.rx32) : nullptr;
@@ -985,6 +1173,18 @@ int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out) {
         if (hs.rmode == R_NONE && hs.cmode == C_NONE) {
           b->broken = true;
           return fail(PDLP_ERR_STATE, "engine: a running LP has no pass scheduled (internal error)");
+        }
+        // iterating (past its first check) and due for the infeasibility test
+        if (sl.detect && hs.cancel == 0 && hs.k >= 64 && hs.k >= sl.next_check) {
+          int request = 0;
+          if ((rc = infeasibility_test(b, sl, &request))) return rc;
+          sl.next_check = hs.k + 256;
+          if (request) {
+            const int req = 100 + request;
+            PDLP_CUDA(cudaMemcpyAsync(&b->d_state[s].cancel, &req, sizeof(int),
+                                      cudaMemcpyHostToDevice, st));
+            PDLP_CUDA(cudaStreamSynchronize(st));
+          }
         }
       }
     }

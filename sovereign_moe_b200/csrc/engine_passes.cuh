@@ -38,7 +38,9 @@ __device__ void begin_iteration(const Inst& I, State* S, bool restart) {
       schedule_final(S, PDLP_STATUS_TIME_LIMIT, src);
       return;
     }
-    if (*(volatile int*)&S->cancel) { schedule_final(S, PDLP_STATUS_INTERRUPTED, src); return; }
+    // a host request to stop: 1 = cancelled (INTERRUPTED), 100 + s = end with status s
+    const int req = *(volatile int*)&S->cancel;
+    if (req) { schedule_final(S, req >= 100 ? req - 100 : PDLP_STATUS_INTERRUPTED, src); return; }
   }
   const int kind = (k % I.stepsize_every == 0) ? P_TRIAL : P_NORMAL;
   S->cprimal = kind;

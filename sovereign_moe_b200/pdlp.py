@@ -51,6 +51,11 @@ class PDLPParams:
     # sparse products, "fp64" (the reference's) or "fp32" (float32 values,
     # directions and row sums; iterates and every check stay float64)
     precision: str = "fp64"
+    # B200 engine only: end an infeasible LP with a certified status (INFEASIBLE,
+    # or INFEASIBLE_OR_UNBOUNDED for a primal ray) instead of running it to its
+    # iteration or time limit; off by default, as the reference has no such test
+    detect_infeasibility: bool = False
+    eps_infeasible: float = 1e-8
 
 
 @dataclass
@@ -125,6 +130,8 @@ def params_struct(params: PDLPParams, n: int, time_used: float = 0.0, history_ca
     if prec not in _lib.PRECISION:
         raise ValueError(f"unknown precision {prec!r}; choose from {sorted(_lib.PRECISION)}")
     p.precision = _lib.PRECISION[prec]
+    p.detect_infeasibility = 1 if getattr(params, "detect_infeasibility", False) else 0
+    p.eps_infeasible = float(getattr(params, "eps_infeasible", 1e-8))
     p.time_used = float(time_used)
     if history_capacity is None:
         history_capacity = int(min(params.max_iter // max(params.check_every, 1) + 1, 1 << 20))

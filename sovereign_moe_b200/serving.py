@@ -80,7 +80,9 @@ class Server:
 
     def __init__(self, max_slots=64, params: PDLPParams | None = None, chunk_steps=64,
                  memory_budget=0, **engine_kw):
-        self.params = params or PDLPParams(device="gpu", eps_abs=1e-6, eps_rel=1e-6)
+        # a served request must end: infeasible and unbounded LPs are detected
+        self.params = params or PDLPParams(device="gpu", eps_abs=1e-6, eps_rel=1e-6,
+                                           detect_infeasibility=True)
         self.engine = BatchEngine(max_slots=max_slots, memory_budget=memory_budget, **engine_kw)
         self.max_slots = int(max_slots)
         self.chunk_steps = int(chunk_steps)
@@ -161,7 +163,8 @@ class Server:
 def serve_one_at_a_time(stream, params: PDLPParams | None = None, realtime=True):
     """The baseline discipline: a FIFO queue, one ``solve_pdlp`` at a time
     (the reference server's behaviour), on the same GPU engine."""
-    params = params or PDLPParams(device="gpu", eps_abs=1e-6, eps_rel=1e-6)
+    params = params or PDLPParams(device="gpu", eps_abs=1e-6, eps_rel=1e-6,
+                                  detect_infeasibility=True)
     reqs = [Request(i, p, float(t) if realtime else 0.0)
             for i, (t, p) in enumerate(sorted(stream, key=lambda e: e[0]))]
     stats = ServeStats()

@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_defaults_match_reference_params():
     lib = _lib.load()
-    assert lib.pdlp_abi_version() == 1
+    assert lib.pdlp_abi_version() == 2
     p = _lib.Params()
     lib.pdlp_params_default(ctypes.byref(p))
     ref = PDLPParams()
@@ -43,6 +43,10 @@ def test_abi_version_and_defaults_match_reference_params():
               "primal_weight_smoothing"):
         assert getattr(p, f) == getattr(ref, f), f
     assert p.scaling == _lib.SCALING["pdlp"]
+    # the fields after the reference's: written by the C default at the same offsets
+    assert p.precision == _lib.PRECISION["fp64"]
+    assert p.detect_infeasibility == 0 and p.eps_infeasible == 1e-8
+    assert ref.detect_infeasibility is False and ref.eps_infeasible == 1e-8
 
 
 def test_struct_layouts_match_the_header():
@@ -50,6 +54,9 @@ def test_struct_layouts_match_the_header():
     assert ctypes.sizeof(_lib.ProblemDesc) == 4 + 4 + 8 + 12 * 8 + 8 + 4 + 4
     assert ctypes.sizeof(_lib.BatchConfig) == 6 * 4 + 8
     assert ctypes.sizeof(_lib.Result) == 8 + 3 * 8 + 9 * 8 + 8 + 8
+    # eps..time_limit, check/stepsize, betas + smoothing, scaling (+pad), power_start,
+    # time_used, history_capacity + precision, detect (+pad), eps_infeasible
+    assert ctypes.sizeof(_lib.Params) == 5 * 8 + 8 + 4 * 8 + 8 + 8 + 8 + 8 + 8 + 8
 
 
 def test_slot_bytes_grows_with_the_problem():

@@ -190,7 +190,10 @@ int pdlp_batch_fetch(pdlp_batch* b, int32_t slot, double* x, double* y,
  * PDLP_SLOT_FREE for an unused slot. */
 #define PDLP_SLOT_FREE -2
 int pdlp_batch_statuses(pdlp_batch* b, int32_t* status_out, int32_t n);
-/* Releases a slot's device memory. */
+/* Releases a slot.  Its device arena is kept for later admissions (best
+ * fit, at most twice the size needed); kept arenas count against the memory
+ * budget, are freed before an admission would be refused, and are freed by
+ * pdlp_batch_destroy. */
 int pdlp_batch_retire(pdlp_batch* b, int32_t slot);
 /* Requests the slot to stop at its next check (status INTERRUPTED). */
 int pdlp_batch_cancel(pdlp_batch* b, int32_t slot);

@@ -42,6 +42,8 @@ extern "C" {
 #define PDLP_ERR_BARRIER_TIMEOUT -4   /* a bounded device wait gave up        */
 #define PDLP_ERR_NUMERICAL       -5   /* non-finite input data                */
 #define PDLP_ERR_STATE           -6   /* call not valid in the handle's state */
+#define PDLP_ERR_BOUNDS          -7   /* an index check failed (bounds-checked
+                                         builds only, -DPDLP_BOUNDS_CHECK)    */
 
 /* ---- statuses: same integers as sovopt Status (src/sovopt/core/problem.py:58-69) */
 #define PDLP_STATUS_OPTIMAL          0

@@ -20,6 +20,7 @@ PDLP_ERR_CUDA = -3
 PDLP_ERR_BARRIER_TIMEOUT = -4
 PDLP_ERR_NUMERICAL = -5
 PDLP_ERR_STATE = -6
+PDLP_ERR_BOUNDS = -7
 
 PDLP_MEM_DEVICE = 0
 PDLP_MEM_HOST = 1

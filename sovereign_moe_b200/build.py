@@ -1,6 +1,7 @@
 """Build ``libpdlp_b200.so`` (the C-ABI engine) in-tree with nvcc for sm_100a.
 
     python -m sovereign_moe_b200.build          # or build() from Python
+    python -m sovereign_moe_b200.build --bounds-check   # checked engine, for test runs
 
 The library links only the CUDA runtime; there is no torch dependency in the
 compiled code.  The output lands next to this file so it travels with the
@@ -39,8 +40,18 @@ def host_compiler() -> list:
     return []
 
 
+STAMP = LIB + ".defines"   # the -D flags the library was built with
+
+
+def _defines(extra) -> str:
+    return " ".join(f for f in (extra or []) if f.startswith("-D"))
+
+
 def _stale() -> bool:
     if not os.path.exists(LIB):
+        return True
+    # a library built with extra defines (a checked build) is rebuilt plain
+    if os.path.exists(STAMP) and open(STAMP).read().strip():
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
@@ -68,9 +79,18 @@ def build(force: bool = False, verbose: bool = False, extra: list | None = None)
     if verbose and (res.stdout or res.stderr):
         print(res.stdout + res.stderr, file=sys.stderr)
     os.replace(LIB + ".tmp", LIB)
+    with open(STAMP, "w") as fh:
+        fh.write(_defines(extra))
     return LIB
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose=True,
-                extra=["-Xptxas", "-v"] if "--ptxas" in sys.argv else None))
+    # --bounds-check: index and row-pointer checks in the engine's tiles
+    # (PDLP_ERR_BOUNDS instead of an out-of-range access), for test runs
+    extra = []
+    if "--ptxas" in sys.argv:
+        extra += ["-Xptxas", "-v"]
+    if "--bounds-check" in sys.argv:
+        extra += ["-DPDLP_BOUNDS_CHECK"]
+    print(build(force="--force" in sys.argv or "--bounds-check" in sys.argv, verbose=True,
+                extra=extra or None))

@@ -1156,7 +1156,11 @@ int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out) {
 #endif
     if (b->h_ctl->error) {
       b->broken = true;
-      return fail(b->h_ctl->error, "engine: a bounded grid barrier timed out; the batch was stopped");
+      if (b->h_ctl->error == PDLP_ERR_BOUNDS)
+        return fail(PDLP_ERR_BOUNDS, "engine: an index check failed in the tile starting at row " +
+                                         std::to_string(b->h_ctl->error_where) +
+                                         "; the batch was stopped");
+      return fail(b->h_ctl->error, "engine: a bounded device wait timed out; the batch was stopped");
     }
     int running = 0;
     for (size_t s = 0; s < b->slots.size(); ++s) {

@@ -113,31 +113,6 @@ struct BulkPhase {
   unsigned m = 0, v = 0;
 };
 
-// ---- asynchronous staging (cp.async, 16-byte, L2 only) -----------------------
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-// Stage elements [first, first + count) of a 16-byte-aligned array of
-// E-byte elements into dst in whole 16-byte chunks; returns the index in dst
-// of element `first`.  The last chunk may read up to 12 bytes past the range
-// (every array of a slot's arena is followed by padding).
-template <int E>
-__device__ __forceinline__ int stage(void* dst, const void* base, int first, int count, int lane) {
-  constexpr int per = 16 / E;
-  const int a = first & ~(per - 1);
-  const int nchunks = (first + count - a + per - 1) / per;
-  const char* src = reinterpret_cast<const char*>(base) + (size_t)a * E;
-  char* d = reinterpret_cast<char*>(dst);
-  for (int c = lane; c < nchunks; c += 32) cp_async16(d + 16 * c, src + 16 * c);
-  return first - a;
-}
-
 // ---- reductions -----------------------------------------------------------
 
 enum : int { OP_SUM = 0, OP_MAX = 1, OP_MIN = 2 };

@@ -214,7 +214,38 @@ __device__ void c_finish(const EngineArgs& A, const Inst& I, State* S, int cmode
 // are in flight, so a pass waits for about two global round trips.  The
 // arithmetic is exactly the generic passes' (same operands, same order).
 
-__device__ __forceinline__ void gather_products(const Tile& t, const double* src, WarpSmem& W,
+// Bounds-checked builds (-DPDLP_BOUNDS_CHECK) test every gathered index
+// against the source vector's length and every staged row pointer against the
+// tile: a failure records PDLP_ERR_BOUNDS (the launch ends at its next grid
+// barrier) and the access is skipped.  Product builds compile none of it.
+#ifdef PDLP_BOUNDS_CHECK
+__device__ __forceinline__ bool index_ok(const EngineArgs& A, int i, int n, int where) {
+  if ((unsigned)i < (unsigned)n) return true;
+  if (atomicCAS(&A.ctl->error, 0, PDLP_ERR_BOUNDS) == 0) A.ctl->error_where = where;
+  return false;
+}
+// The staged row pointers of a normal tile: start at the tile's first entry,
+// never decrease, and end at its last.
+__device__ __forceinline__ bool tile_ptrs_ok(const EngineArgs& A, const Tile& t, const int* tptr,
+                                             int lane) {
+  const int rows = t.end - t.begin;
+  bool ok = true;
+  for (int i = lane; i < rows; i += 32) ok &= tptr[i] <= tptr[i + 1];
+  if (lane == 0) ok &= tptr[0] == t.p0 && tptr[rows] == t.p0 + t.cnt;
+  ok = __all_sync(0xffffffffu, ok);
+  if (!ok && lane == 0 && atomicCAS(&A.ctl->error, 0, PDLP_ERR_BOUNDS) == 0)
+    A.ctl->error_where = t.begin;
+  return ok;
+}
+#else
+__device__ __forceinline__ bool index_ok(const EngineArgs&, int, int, int) { return true; }
+__device__ __forceinline__ bool tile_ptrs_ok(const EngineArgs&, const Tile&, const int*, int) {
+  return true;
+}
+#endif
+
+__device__ __forceinline__ void gather_products(const EngineArgs& A, const Tile& t,
+                                                const double* src, int len, WarpSmem& W,
                                                 int offi, int offv, int lane) {
   double* prod = W.sval + offv;
   const int* idx = W.sidx + offi;
@@ -223,7 +254,7 @@ __device__ __forceinline__ void gather_products(const Tile& t, const double* src
 #pragma unroll
   for (int u = 0; u < kWTileNnz / 32; ++u) {
     const int q = lane + 32 * u;
-    g[u] = q < cnt ? ld_gather(src + idx[q]) : 0.0;
+    g[u] = (q < cnt && index_ok(A, idx[q], len, t.begin)) ? ld_gather(src + idx[q]) : 0.0;
   }
 #pragma unroll
   for (int u = 0; u < kWTileNnz / 32; ++u) {
@@ -233,7 +264,8 @@ __device__ __forceinline__ void gather_products(const Tile& t, const double* src
   __syncwarp();
 }
 
-__device__ __forceinline__ void gather_products_f32(const Tile& t, const float* src, WarpSmem& W,
+__device__ __forceinline__ void gather_products_f32(const EngineArgs& A, const Tile& t,
+                                                    const float* src, int len, WarpSmem& W,
                                                     int offi, int offv, int lane) {
   float* prod = reinterpret_cast<float*>(W.sval) + offv;
   const int* idx = W.sidx + offi;
@@ -242,7 +274,7 @@ __device__ __forceinline__ void gather_products_f32(const Tile& t, const float* 
 #pragma unroll
   for (int u = 0; u < kWTileNnz / 32; ++u) {
     const int q = lane + 32 * u;
-    g[u] = q < cnt ? ld_gather(src + idx[q]) : 0.0f;
+    g[u] = (q < cnt && index_ok(A, idx[q], len, t.begin)) ? ld_gather(src + idx[q]) : 0.0f;
   }
 #pragma unroll
   for (int u = 0; u < kWTileNnz / 32; ++u) {
@@ -306,14 +338,15 @@ __device__ void hot_rtile(const EngineArgs& A, const Tile& t, int ti, const Inst
   const int off = bulk_offset<8>(t.begin);
   HOT_STAMP(1);
   if (!bulk_wait(A, &W.bar[0], ph.m)) { bulk_wait(A, &W.bar[1], ph.v); return; }
+  if (!tile_ptrs_ok(A, t, W.sptr + offp, lane)) { bulk_wait(A, &W.bar[1], ph.v); return; }
   HOT_STAMP(2);
   if (I.f32) {
-    gather_products_f32(t, I.dx32, W, offi, offv, lane);
+    gather_products_f32(A, t, I.dx32, I.n, W, offi, offv, lane);
     HOT_STAMP(3);
     staged_row_sums_f32(W.sptr + offp, reinterpret_cast<const float*>(W.sval) + offv, rows,
                         I.lanes_r, W.s0, lane);
   } else {
-    gather_products(t, I.dx, W, offi, offv, lane);
+    gather_products(A, t, I.dx, I.n, W, offi, offv, lane);
     HOT_STAMP(3);
     staged_row_sums(W.sptr + offp, W.sval + offv, rows, I.lanes_r, W.s0, lane);
   }
@@ -405,12 +438,13 @@ __device__ void hot_ctile(const EngineArgs& A, const Tile& t, int ti, const Inst
   const int off = bulk_offset<8>(t.begin);
   if (iter) {     // only the iteration staged the matrix (the primal step needs none)
     if (!bulk_wait(A, &W.bar[0], ph.m)) { bulk_wait(A, &W.bar[1], ph.v); return; }
+    if (!tile_ptrs_ok(A, t, W.sptr + offp, lane)) { bulk_wait(A, &W.bar[1], ph.v); return; }
     if (I.f32) {
-      gather_products_f32(t, I.dy32, W, offi, offv, lane);
+      gather_products_f32(A, t, I.dy32, I.m, W, offi, offv, lane);
       staged_row_sums_f32(W.sptr + offp, reinterpret_cast<const float*>(W.sval) + offv, rows,
                           I.lanes_c, W.s0, lane);
     } else {
-      gather_products(t, I.dy, W, offi, offv, lane);
+      gather_products(A, t, I.dy, I.m, W, offi, offv, lane);
       staged_row_sums(W.sptr + offp, W.sval + offv, rows, I.lanes_c, W.s0, lane);
     }
   }
@@ -500,6 +534,7 @@ __device__ void process_rtile(const EngineArgs& A, const Tile t, int ti, WarpSme
   if (!t.heavy && !bulk_wait(A, &W.bar[0], ph.m)) return;
   __syncwarp();
   const int* tptr = W.sptr + offp;
+  if (!t.heavy && !tile_ptrs_ok(A, t, tptr, lane)) return;
 
   const int L = I.lanes_r;
   const int* __restrict__ rp = I.rp;
@@ -996,6 +1031,7 @@ __device__ void process_ctile(const EngineArgs& A, const Tile t, int ti, WarpSme
   if (!t.heavy && !bulk_wait(A, &W.bar[0], ph.m)) return;
   __syncwarp();
   const int* tptr = W.sptr + offp;
+  if (!t.heavy && !tile_ptrs_ok(A, t, tptr, lane)) return;
 
   const int L = I.lanes_c;
   const int* __restrict__ cp = I.cp;

@@ -320,6 +320,17 @@ def verify_batch(arm, lps):
     return worst
 
 
+def rank_max(v, world, device="cuda"):
+    """The maximum of ``v`` over the ranks (the timing rule for N > 1)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_gpu(args, rank, world):
     import torch
     import torch.distributed as dist
@@ -345,11 +356,7 @@ def run_gpu(args, rank, world):
         torch.cuda.synchronize()
 
     def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(v, world, "cuda")
 
     # device-resident timing
     clocks = ClockSampler(local)

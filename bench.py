@@ -48,8 +48,8 @@ EPS = 1e-6
 # DRAM bytes per algorithmic byte of engine_persistent on this batch, from one
 # ncu capture of the second 256-step launch of
 # `bench.py --workload engine-steps --iters 512`: dram__bytes_read.sum +
-# dram__bytes_write.sum = 93.90 GB against 87.55 GB of algorithmic bytes.
-TRAFFIC_PER_ALGORITHMIC_BYTE = 93.90 / 87.55
+# dram__bytes_write.sum = 93.34 GB against 87.55 GB of algorithmic bytes.
+TRAFFIC_PER_ALGORITHMIC_BYTE = 93.34 / 87.55
 
 
 def load_peaks():

@@ -15,9 +15,6 @@ namespace pdlp {
 
 // ---- grid barrier (bounded) ----------------------------------------------------
 //
-// Arrive with a fenced atomic, wait for the generation to flip.  The wait is
-// bounded in wall time: on timeout the block records PDLP_ERR_BARRIER_TIMEOUT
-// in the control block and every block leaves the kernel at its next barrier.
 // Grid barrier on a monotonic arrival counter: the k-th barrier of a launch
 // is passed once the counter reaches k * nblocks (the host zeroes it before
 // each launch).  Arrival is an acquire-release add, the wait an acquire load,

@@ -209,10 +209,11 @@ __device__ void c_finish(const EngineArgs& A, const Inst& I, State* S, int cmode
 // ---- hot modes: staged tile passes ------------------------------------------
 //
 // The iteration (R_ITER, C_ITER), line-search trial (R_TRIAL) and primal step
-// (C_PRIMAL) passes run from shared memory: the tile's matrix arrays were
-// staged by the caller; here the epilogue vectors are staged while the gathers
-// are in flight, so a pass waits for about two global round trips.  The
-// arithmetic is exactly the generic passes' (same operands, same order).
+// (C_PRIMAL) passes run from shared memory.  The caller has issued the bulk
+// copies of the tile's matrix arrays; here one lane issues those of the
+// epilogue vectors, which land while the gathers are in flight, so a pass
+// waits for about two global round trips.  The arithmetic is exactly the
+// generic passes' (same operands, same order).
 
 // Bounds-checked builds (-DPDLP_BOUNDS_CHECK) test every gathered index
 // against the source vector's length and every staged row pointer against the

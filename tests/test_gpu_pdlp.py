@@ -229,3 +229,55 @@ def test_cancel_ends_as_interrupted(require_gpu):
     assert ra.iterations < 100_000
     assert rb.status == Status.OPTIMAL
     assert abs(rb.objective - float(exp_b.known)) / max(1.0, abs(float(exp_b.known))) < 1e-6
+
+
+def _edge_lp(name):
+    from sovereign_moe_b200.problem import INF, Problem, SparseMatrix
+
+    def lp(rows, cols, vals, m, n, c, rl, ru, lo, hi):
+        A = SparseMatrix.from_triplets(np.array(rows, dtype=np.int64),
+                                       np.array(cols, dtype=np.int64),
+                                       np.array(vals, float), m, n)
+        return Problem(A=A, c=np.array(c, float), row_lb=np.array(rl, float),
+                       row_ub=np.array(ru, float), col_lb=np.array(lo, float),
+                       col_ub=np.array(hi, float))
+    return {
+        "no_rows": lp([], [], [], 0, 3, [1, -1, 2], [], [], [0, 0, -1], [5, 4, 3]),
+        "empty_row": lp([0, 0], [0, 1], [1, 1], 2, 2, [1, 1], [1, -1], [INF, 1],
+                        [0, 0], [10, 10]),
+        "empty_column": lp([0, 0], [0, 1], [1, 1], 1, 3, [1, 1, -2], [1], [INF],
+                           [0, 0, 0], [10, 10, 7]),
+        "one_by_one": lp([0], [0], [2.0], 1, 1, [3.0], [4.0], [4.0], [0], [INF]),
+    }[name]
+
+
+@pytest.mark.parametrize("name", ["no_rows", "empty_row", "empty_column", "one_by_one"])
+def test_edge_shapes_match_oracle(require_gpu, name):
+    """LPs with no rows, an empty row, an empty column, one entry: the same
+    status, iterate and objective as the reference restated in the oracle."""
+    from oracle import pdlp_oracle as po
+    prob = _edge_lp(name)
+    ref = po.solve_pdlp(prob, dict(eps_abs=1e-8, eps_rel=1e-8))
+    s = solve_pdlp(prob, PDLPParams(device="gpu"))
+    assert int(s.status) == int(ref.status)
+    assert s.iterations == ref.iterations
+    np.testing.assert_allclose(s.x, ref.x, rtol=1e-9, atol=1e-9)
+    assert abs(s.objective - ref.objective) <= 1e-9 * max(1.0, abs(ref.objective))
+
+
+def test_sizes_beyond_int32_entries_are_refused(require_gpu):
+    """The engine indexes entries with int32: a problem whose nnz does not fit
+    is refused at admission with PDLP_ERR_ARG, before any device work."""
+    import ctypes
+    from sovereign_moe_b200 import _lib
+    from sovereign_moe_b200.batch import BatchEngine
+    with BatchEngine(max_slots=1) as eng:
+        d = _lib.ProblemDesc()
+        d.m, d.n, d.nnz = 10, 10, 1 << 31
+        d.sense, d.memory = 1, _lib.PDLP_MEM_HOST
+        p = _lib.Params()
+        eng.lib.pdlp_params_default(ctypes.byref(p))
+        slot = ctypes.c_int32(-1)
+        code = eng.lib.pdlp_batch_admit(eng.h, ctypes.byref(d), ctypes.byref(p), ctypes.byref(slot))
+        assert code == _lib.PDLP_ERR_ARG
+        assert "int32" in eng.lib.pdlp_last_error().decode()

@@ -594,6 +594,113 @@ def run_spmv(args):
     return 0
 
 
+def bnr_bytes_per_iteration(m, n, nnz, K):
+    """Algorithmic HBM bytes of one batched PDHG iteration over K nodes: each
+    (rows, K) float64 block read or written once per kernel that touches it
+    (primal 6 n-blocks, A dX 1 n + 1 m, dual 5 m, A^T dY 1 m + 1 n, sums 2 m +
+    1 n, updates 5 n + 5 m), plus the CSR and CSC matrices once each."""
+    return 8 * 14 * (m + n) * K + 2 * (12 * nnz + 8 * (max(m, n) + 1))
+
+
+def run_bnr(args):
+    """Batched node relaxation (``sovereign_moe_b200.bnr.BNREngine``, the
+    reference's ``sovopt.mip.bnr``): 128 nodes of a 20,000 x 30,000 LP (8 nnz
+    per column), 60 PDHG iterations and a safe dual bound per node per call.
+    Metric: node bounds per second.  ``value``: one call on device-resident
+    bound sets and outputs, L2 flushed (256 MB write) before each; ``e2e``:
+    the public ``solve_batch`` with pinned host arrays in and bounds, x and y
+    back; ``one_at_a_time``: the same 128 nodes as 128 calls of one node (a
+    conventional tree's order); ``cpu_baseline``: the oracle restatement of
+    the reference's CPU engine on the same batch, timed over a few iterations
+    and scaled to 60."""
+    import torch
+    from types import SimpleNamespace
+    from sovereign_moe_b200 import _lib
+    from sovereign_moe_b200.bnr import BNRConfig, BNREngine
+    from sovereign_moe_b200.workloads import node_relaxation
+    peak, kind = load_peaks()
+    K, iters = 128, 60
+    prob, L, U = node_relaxation(nodes=K)
+    m, n, nnz = prob.A.m, prob.A.n, prob.A.nnz
+    sc = SimpleNamespace(obj=1.0)
+    eng = BNREngine(prob, sc, BNRConfig(batch=K, iters=iters, device="gpu"))
+    lib = eng.lib
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    dev = lambda a: torch.as_tensor(a, device="cuda").contiguous()  # noqa: E731
+    dL, dU = dev(L), dev(U)
+    dbounds = torch.empty(K, dtype=torch.float64, device="cuda")
+    dx = torch.empty((n, K), dtype=torch.float64, device="cuda")
+    dy = torch.empty((m, K), dtype=torch.float64, device="cuda")
+    dinf = torch.empty(K, dtype=torch.uint8, device="cuda")
+
+    def device_call():
+        _lib.check(lib.pdlp_bnr_solve_batch(eng.h, K, dL.data_ptr(), dU.data_ptr(), None, None,
+                                            iters, 0.3, 0.6, dbounds.data_ptr(), dx.data_ptr(),
+                                            dy.data_ptr(), dinf.data_ptr(), _lib.PDLP_MEM_DEVICE))
+
+    def timed(fn, steps):
+        out = []
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = _sync_events(torch)
+            torch.cuda.synchronize()
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            out.append(e0.elapsed_time(e1))
+        return out
+
+    for _ in range(max(3, args.warmup)):
+        device_call()
+    n0 = lib.pdlp_launch_count()
+    dev_ms = timed(device_call, args.steps)
+    launches = (lib.pdlp_launch_count() - n0) // max(1, args.steps)
+    # e2e through the public API, pinned host buffers
+    pin = lambda a: torch.as_tensor(a).pin_memory().numpy()  # noqa: E731
+    hL, hU = pin(L), pin(U)
+    for _ in range(3):
+        eng.solve_batch(hL, hU)
+    e2e_ms = timed(lambda: eng.solve_batch(hL, hU), args.steps)
+    # one node at a time: 128 calls of K = 1
+    one = BNREngine(prob, sc, BNRConfig(batch=1, iters=iters, device="gpu"))
+    cols = [(np.ascontiguousarray(L[:, k:k + 1]), np.ascontiguousarray(U[:, k:k + 1]))
+            for k in range(K)]
+    for k in range(3):
+        one.solve_batch(*cols[k])
+    one_ms = timed(lambda: [one.solve_batch(*c) for c in cols], 1)[0]
+    ms = statistics.median(dev_ms)
+    it_bytes = bnr_bytes_per_iteration(m, n, nnz, K)
+    gbps = it_bytes * iters / ms / 1e6
+    line = {"metric": "BNR node bounds/s", "unit": "nodes/s", "value": K / ms * 1e3,
+            "ms_per_step": ms, "steps": args.steps, "warmup": max(3, args.warmup),
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"node_relaxation_{m}x{n}", "nnz": int(nnz), "nodes": K,
+                       "iterations": iters, "l2": "flushed before every call (256 MB write)"},
+            "gpu_launches": int(launches),
+            "e2e": {"value": K / statistics.median(e2e_ms) * 1e3, "unit": "nodes/s",
+                    "ms_per_step": statistics.median(e2e_ms),
+                    "h2d_bytes_per_step": int(L.nbytes + U.nbytes),
+                    "d2h_bytes_per_step": int(8 * K + 8 * n * K + 8 * m * K + K)},
+            "one_at_a_time": {"value": K / one_ms * 1e3, "unit": "nodes/s", "ms": one_ms},
+            "roofline": {"bound": "hbm", "achieved": gbps, "peak": peak, "unit": "GB/s",
+                         "frac": gbps / peak, "peak_source": kind,
+                         "algorithmic_bytes_per_iteration": it_bytes,
+                         "note": "whole call (60 iterations + bound) against the iterations' bytes"}}
+    if not args.no_cpu:
+        import oracle.bnr_oracle as bo
+        A = prob.A
+        o = bo.BNROracle(A.rp, A.ri, A.rx, A.cp, A.ci, A.cx, prob.c, prob.row_lb, prob.row_ub,
+                         1.0, 0.0, batch=K, iters=4)
+        t0 = time.perf_counter()
+        o.solve_batch(L, U)
+        t = (time.perf_counter() - t0) * iters / 4
+        line["cpu_baseline"] = {"value": K / t, "unit": "nodes/s", "cores": 1, "kind": "port",
+                                "sample": f"{K} nodes x 4 iterations (+ bound), scaled to {iters}"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_precision(args):
     """FP32-SpMV against float64 per instance: config-1-shaped known-optimum
     LPs (230 x 2025, seeds 0-7) and 8 LPs of the uneven batch, each solved at
@@ -658,7 +765,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="batch",
                     choices=["batch", "blend", "powerlaw", "serving", "engine-steps", "spmv",
-                             "precision"],
+                             "precision", "bnr"],
                     help="batch: the headline metric; the others print auxiliary lines")
     ap.add_argument("--iters", type=int, default=2000)
     ap.add_argument("--scale", type=float, default=1.0)
@@ -680,6 +787,8 @@ def main():
         return run_spmv(args)
     if args.workload == "precision":
         return run_precision(args)
+    if args.workload == "bnr":
+        return run_bnr(args)
     if args.warmup < 3 and args.impl == "ours":
         ap.error("--warmup must be >= 3")
     rank = int(os.environ.get("RANK", "0"))

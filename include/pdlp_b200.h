@@ -244,6 +244,33 @@ int pdlp_pdhg_accum(int32_t n, double* acc, const double* inc, double* run_sum,
 int pdlp_dot(int64_t n, const double* a, const double* b, double* out, void* stream);
 int pdlp_nrm2(int64_t n, const double* a, double* out, void* stream);
 int pdlp_nrm_inf(int64_t n, const double* a, double* out, void* stream);
+/* ---- batched node relaxation (mip/bnr.py:176-301) ----------------------- *
+ * K node LPs that share one pdlp-scaled problem (matrix, costs, row bounds)
+ * and differ only in column bounds, advanced together by a fixed number of
+ * PDHG iterations with a step size per node, then bounded by each node's safe
+ * dual bound (mip/safebound.py:194-235).  Node blocks are (rows, K) with the
+ * node index fastest, so each sparse product reads A once for all K nodes. */
+typedef struct pdlp_bnr pdlp_bnr;
+/* BNREngine.__init__ (bnr.py:128-151): the scaled problem (CSR and CSC of A,
+ * c, row bounds, obj_offset; col bounds and kind unused) and the objective
+ * scale; node buffers for max_batch nodes, grown on demand. */
+int pdlp_bnr_create(const pdlp_problem_desc* scaled, double obj_scale, int32_t max_batch,
+                    void* stream, pdlp_bnr** out);
+int pdlp_bnr_destroy(pdlp_bnr* b);
+/* BNREngine.solve_batch: col_lb / col_ub (n, K); warm_x (n, K) and warm_y
+ * (m, K) or both NULL (start at 0); iters iterations with step exponents
+ * step_growth / step_damp (BNRConfig: 0.3 / 0.6).  Outputs, each optional:
+ * bounds[K] in the original objective scale (+inf for an empty box, -inf
+ * when the duals certify nothing), x (n, K), y (m, K), infeasible[K] (1 for
+ * an empty box).  Pointers in `memory`.  The step sizes persist in the
+ * engine between calls, as in the reference. */
+int pdlp_bnr_solve_batch(pdlp_bnr* b, int32_t K, const double* col_lb, const double* col_ub,
+                         const double* warm_x, const double* warm_y, int32_t iters,
+                         double step_growth, double step_damp, double* bounds, double* x,
+                         double* y, uint8_t* infeasible, int32_t memory);
+/* The engine's current step sizes of the first K nodes (host arrays). */
+int pdlp_bnr_step_sizes(pdlp_bnr* b, int32_t K, double* eta, double* omega);
+
 /* a . b to a host double, like pdlp_dot, but without allocating any device
  * memory.  No counterpart in the reference.  It is for callers that must not
  * allocate: a serving loop that has given the free device memory to resident

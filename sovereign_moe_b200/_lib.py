@@ -108,6 +108,12 @@ SIGNATURES = {
     "pdlp_dot": ([_i64, _c_p, _c_p, ctypes.POINTER(_d), _c_p], ctypes.c_int),
     "pdlp_nrm2": ([_i64, _c_p, ctypes.POINTER(_d), _c_p], ctypes.c_int),
     "pdlp_nrm_inf": ([_i64, _c_p, ctypes.POINTER(_d), _c_p], ctypes.c_int),
+    "pdlp_bnr_create": ([ctypes.POINTER(ProblemDesc), _d, _i32, _c_p, ctypes.POINTER(_c_p)],
+                        ctypes.c_int),
+    "pdlp_bnr_destroy": ([_c_p], ctypes.c_int),
+    "pdlp_bnr_solve_batch": ([_c_p, _i32, _c_p, _c_p, _c_p, _c_p, _i32, _d, _d, _c_p, _c_p,
+                              _c_p, _c_p, _i32], ctypes.c_int),
+    "pdlp_bnr_step_sizes": ([_c_p, _i32, _c_p, _c_p], ctypes.c_int),
     "pdlp_dot_noalloc": ([_i64, _c_p, _c_p, ctypes.POINTER(_d), _c_p], ctypes.c_int),
 }
 

@@ -176,6 +176,36 @@ def uneven_batch(seed=0, count=256, m_lo=50, m_hi=5000):
     return out
 
 
+def node_relaxation(seed=1234, m=20_000, n=30_000, per_col=8, nodes=128):
+    """A 20,000 x 30,000 LP with 8 nnz per column (uniform random rows,
+    N(0,1) values) around an interior point x0 ~ U[0,1): rows A x = A x0,
+    costs N(0,1), columns in [0, 10] -- the matrix shape the reference
+    benchmarks batched node relaxation on (bench/gpu_bench.py:31-44, 173).
+    There the rows are A x <= A x0 + U[0, 0.5); here they are equalities,
+    because the reference's safe dual bound (safebound.py:212-230) prices a
+    positive dual at the row's lower bound and a negative one at its upper
+    bound, while its PDHG step (bnr.py:238-242) gives a one-sided row the
+    dual sign whose price is infinite, so every bound of that LP would be
+    -inf.  Also ``nodes`` branch-and-bound-like bound sets (n, nodes): node k
+    halves the box of 3 random columns.  Returns (problem, L, U)."""
+    rng = np.random.default_rng(seed)
+    cp, ci = random_structure(rng, m, np.full(n, per_col))
+    cx = rng.standard_normal(ci.shape[0])
+    A = SparseMatrix(m, n, cp, ci, cx)
+    x0 = rng.random(n)
+    b = A.matvec(x0)
+    prob = Problem(A=A, c=rng.standard_normal(n), row_lb=b, row_ub=b.copy(),
+                   col_lb=np.zeros(n), col_ub=np.full(n, 10.0), name=f"nodes_{m}x{n}")
+    L = np.zeros((n, nodes))
+    U = np.full((n, nodes), 10.0)
+    for k in range(nodes):
+        j = rng.choice(n, size=3, replace=False)
+        lower = rng.random(3) < 0.5
+        U[j[lower], k] = 5.0
+        L[j[~lower], k] = 5.0
+    return prob, L, U
+
+
 def power_law(seed=0, m=1_000_000, n=3_000_000, nnz=10_000_000, alpha=1.5,
               cap=2000, heavy_rows=0.01, heavy_scale=1e4):
     """Zipf(alpha) column degrees capped at ``cap`` and rescaled so they sum to

@@ -47,6 +47,16 @@ class BatchResult:
     y: np.ndarray | None = None
 
 
+class _HostView:
+    """``engine.bk`` for callers written against the reference engine, which
+    read ``engine.bk.to_host(engine.Y[:, :K])`` (mip/tree.py:1025): the
+    iterates this engine returns are already host arrays."""
+
+    @staticmethod
+    def to_host(a):
+        return np.asarray(a)
+
+
 class BNREngine:
     """Holds the shared scaled problem on the device and advances node batches."""
 
@@ -81,6 +91,8 @@ class BNREngine:
             raise RuntimeError(f"GPU backend unavailable ({self.lib.pdlp_last_error().decode()})")
         _lib.check(code)
         self.h = h
+        self.bk = _HostView()
+        self._cap = max(1, int(self.cfg.batch))
         self.total_iterations = 0
         self.total_batches = 0
         self.total_nodes = 0
@@ -102,6 +114,15 @@ class BNREngine:
         """The dual iterates (m, K) of the last batch (the reference keeps them
         on its engine; its tree caches them as warm starts)."""
         return self._last_y
+
+    @property
+    def eta(self):
+        """Step sizes of every node slot (bnr.py:168-171)."""
+        return self.step_sizes(self._cap)[0]
+
+    @property
+    def omega(self):
+        return self.step_sizes(self._cap)[1]
 
     def step_sizes(self, K):
         eta = np.empty(K)
@@ -138,6 +159,8 @@ class BNREngine:
             bounds.ctypes.data, x.ctypes.data, y.ctypes.data, inf.ctypes.data,
             _lib.PDLP_MEM_HOST))
         self._last_y = y
+        if K > self._cap:
+            self._cap = max(K, 2 * self._cap)
         self.total_iterations += self.cfg.iters
         self.total_batches += 1
         self.total_nodes += K

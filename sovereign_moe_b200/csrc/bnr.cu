@@ -7,9 +7,9 @@
 //
 // Layout: every per-node block is (rows, K) with the node index fastest, so a
 // sparse product reads A once for all K nodes (A X with X (n, K)).  One
-// iteration is eight launches:
-//   primal step  ->  A dX  ->  dual step  ->  A^T dY  ->  per-node sums
-//   -> per-node accept / step size  ->  n-side and m-side updates.
+// iteration is seven launches:
+//   primal step (+ sum dX dX)  ->  A dX  ->  dual step (+ sums dY AdX, dY dY)
+//   ->  A^T dY  ->  per-node accept / step size  ->  n-side and m-side updates.
 // The iterations of one call are captured once into a CUDA graph, keyed by
 // (K, iterations, step exponents), and replayed.
 //
@@ -64,70 +64,16 @@ __global__ void __launch_bounds__(256) bnr_spmm(int rows, int k, const int64_t* 
   Y[g] = acc;
 }
 
-// Xn = clip(X - tau (c + AtY), L, U), dX = Xn - X   (bnr.py:233-236)
-__global__ void bnr_primal(long long total, int k, const double* __restrict__ c,
-                           const double* __restrict__ eta, const double* __restrict__ omega,
-                           const double* __restrict__ X, const double* __restrict__ AtY,
-                           const double* __restrict__ L, const double* __restrict__ U,
-                           double* __restrict__ Xn, double* __restrict__ dX) {
-  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= total) return;
-  const int node = (int)(g % k);
-  const double tau = eta[node] / omega[node];
-  const double xn = clipd(sub(X[g], mul(tau, add(c[g / k], AtY[g]))), L[g], U[g]);
-  Xn[g] = xn;
-  dX[g] = sub(xn, X[g]);
-}
-
-// W = Y + sigma (AX + 2 AdX); Yn = W - sigma clip(W / sigma, rl, ru); dY = Yn - Y
-// (bnr.py:238-242)
-__global__ void bnr_dual(long long total, int k, const double* __restrict__ rl,
-                         const double* __restrict__ ru, const double* __restrict__ eta,
-                         const double* __restrict__ omega, const double* __restrict__ Y,
-                         const double* __restrict__ AX, const double* __restrict__ AdX,
-                         double* __restrict__ Yn, double* __restrict__ dY) {
-  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= total) return;
-  const int node = (int)(g % k);
-  const long long i = g / k;
-  const double sigma = eta[node] * omega[node];
-  const double w = add(Y[g], mul(sigma, add(AX[g], mul(2.0, AdX[g]))));
-  const double yn = sub(w, mul(sigma, clipd(w / sigma, rl[i], ru[i])));
-  Yn[g] = yn;
-  dY[g] = sub(yn, Y[g]);
-}
-
-// Per-node partial sums over a block of kRowsPerBlock rows.  Blocks
-// [0, mblocks) cover the m side and give (sum dY AdX, sum dY dY); blocks
-// [mblocks, mblocks + nblocks) cover the n side and give sum dX dX.  Block
-// (32, 8): threadIdx.x is the node within a 32-node tile, threadIdx.y the row
-// phase; a fixed tree combines the 8 phases.  Output pair of row block b and
-// node j at part[2 (b k + j)].
-__global__ void __launch_bounds__(256) bnr_sums(int m, int n, int k, int mblocks,
-                                                const double* __restrict__ dY,
-                                                const double* __restrict__ AdX,
-                                                const double* __restrict__ dX,
-                                                double* __restrict__ part) {
+// The per-node sums over rows run in a fixed order: blocks of kRowsPerBlock
+// rows; in a block, phase y (threadIdx.y, 8 phases) adds rows r0 + y + 8 j
+// for j ascending from 0.0; the phases are added in order; bnr_accept adds
+// the blocks in order.  The element-wise kernels below walk their rows in that
+// layout, block (32, 8) with threadIdx.x the node within a 32-node tile, and
+// sum as they go.  Output pair of row block b and node j at part[2 (b k + j)]:
+// m-side blocks [0, mblocks), n-side blocks [mblocks, mblocks + nblocks).
+__device__ __forceinline__ void bnr_block_sums(double s0, double s1, int k, int node,
+                                               long long part_block, double* __restrict__ part) {
   __shared__ double sh[2][8][32];
-  const bool mside = (int)blockIdx.x < mblocks;
-  const int b = mside ? blockIdx.x : blockIdx.x - mblocks;
-  const int rows = mside ? m : n;
-  const int node = blockIdx.y * 32 + threadIdx.x;
-  double s0 = 0.0, s1 = 0.0;
-  if (node < k) {
-    const int r0 = b * kRowsPerBlock, r1 = min(rows, r0 + kRowsPerBlock);
-    for (int r = r0 + threadIdx.y; r < r1; r += 8) {
-      const long long g = (long long)r * k + node;
-      if (mside) {
-        const double d = dY[g];
-        s0 = add(s0, mul(d, AdX[g]));
-        s1 = add(s1, mul(d, d));
-      } else {
-        const double d = dX[g];
-        s0 = add(s0, mul(d, d));
-      }
-    }
-  }
   sh[0][threadIdx.y][threadIdx.x] = s0;
   sh[1][threadIdx.y][threadIdx.x] = s1;
   __syncthreads();
@@ -137,10 +83,71 @@ __global__ void __launch_bounds__(256) bnr_sums(int m, int n, int k, int mblocks
       a = add(a, sh[0][y][threadIdx.x]);
       c2 = add(c2, sh[1][y][threadIdx.x]);
     }
-    double* out = part + ((long long)blockIdx.x * k + node) * 2;
+    double* out = part + (part_block * k + node) * 2;
     out[0] = a;
     out[1] = c2;
   }
+}
+
+// Xn = clip(X - tau (c + AtY), L, U), dX = Xn - X (bnr.py:233-236), and the
+// node's sum of dX dX over the block's rows.
+__global__ void __launch_bounds__(256) bnr_primal(int n, int k, int mblocks,
+                                                  const double* __restrict__ c,
+                                                  const double* __restrict__ eta,
+                                                  const double* __restrict__ omega,
+                                                  const double* __restrict__ X,
+                                                  const double* __restrict__ AtY,
+                                                  const double* __restrict__ L,
+                                                  const double* __restrict__ U,
+                                                  double* __restrict__ Xn, double* __restrict__ dX,
+                                                  double* __restrict__ part) {
+  const int node = blockIdx.y * 32 + threadIdx.x;
+  double s = 0.0;
+  if (node < k) {
+    const double tau = eta[node] / omega[node];
+    const int r0 = blockIdx.x * kRowsPerBlock, r1 = min(n, r0 + kRowsPerBlock);
+    for (int r = r0 + threadIdx.y; r < r1; r += 8) {
+      const long long g = (long long)r * k + node;
+      const double x = X[g];
+      const double xn = clipd(sub(x, mul(tau, add(__ldg(c + r), AtY[g]))), L[g], U[g]);
+      const double d = sub(xn, x);
+      Xn[g] = xn;
+      dX[g] = d;
+      s = add(s, mul(d, d));
+    }
+  }
+  bnr_block_sums(s, 0.0, k, node, (long long)mblocks + blockIdx.x, part);
+}
+
+// W = Y + sigma (AX + 2 AdX); Yn = W - sigma clip(W / sigma, rl, ru); dY = Yn - Y
+// (bnr.py:238-242), and the node's sums of dY AdX and dY dY over the block's rows.
+__global__ void __launch_bounds__(256) bnr_dual(int m, int k, const double* __restrict__ rl,
+                                                const double* __restrict__ ru,
+                                                const double* __restrict__ eta,
+                                                const double* __restrict__ omega,
+                                                const double* __restrict__ Y,
+                                                const double* __restrict__ AX,
+                                                const double* __restrict__ AdX,
+                                                double* __restrict__ Yn, double* __restrict__ dY,
+                                                double* __restrict__ part) {
+  const int node = blockIdx.y * 32 + threadIdx.x;
+  double s0 = 0.0, s1 = 0.0;
+  if (node < k) {
+    const double sigma = eta[node] * omega[node];
+    const int r0 = blockIdx.x * kRowsPerBlock, r1 = min(m, r0 + kRowsPerBlock);
+    for (int r = r0 + threadIdx.y; r < r1; r += 8) {
+      const long long g = (long long)r * k + node;
+      const double y = Y[g], adx = AdX[g];
+      const double w = add(y, mul(sigma, add(AX[g], mul(2.0, adx))));
+      const double yn = sub(w, mul(sigma, clipd(w / sigma, __ldg(rl + r), __ldg(ru + r))));
+      const double d = sub(yn, y);
+      Yn[g] = yn;
+      dY[g] = d;
+      s0 = add(s0, mul(d, adx));
+      s1 = add(s1, mul(d, d));
+    }
+  }
+  bnr_block_sums(s0, s1, k, node, blockIdx.x, part);
 }
 
 // Per node: the sums in block order, then the step test and the next step size
@@ -313,6 +320,7 @@ struct pdlp_bnr {
   cudaGraphExec_t graph = nullptr;
   double* fac = nullptr;          // per iteration (1 - t^-growth, 1 + t^-damp)
   int g_k = -1, g_iters = -1;
+  long long g_launches = 0;
   double g_growth = 0.0, g_damp = 0.0;
 };
 
@@ -370,25 +378,32 @@ int bnr_upload(T** dst, const T* src, size_t count, int memory, cudaStream_t st)
   return PDLP_OK;
 }
 
-// The launches of `iters` iterations for K nodes, on stream s.
-void bnr_enqueue_iterations(pdlp_bnr* b, int K, int iters, cudaStream_t s) {
+// The launches of `iters` iterations for K nodes, on stream s; returns how
+// many kernels it launched.
+long long bnr_enqueue_iterations(pdlp_bnr* b, int K, int iters, cudaStream_t s) {
   const long long nk = (long long)b->n * K, mk = (long long)b->m * K;
   const int mblocks = (b->m + kRowsPerBlock - 1) / kRowsPerBlock;
   const int nblocks = (b->n + kRowsPerBlock - 1) / kRowsPerBlock;
-  const dim3 sgrid(std::max(1, mblocks + nblocks), (K + 31) / 32), sblock(32, 8);
+  const dim3 tb(32, 8);
+  const dim3 ngrid(std::max(1, nblocks), (K + 31) / 32), mgrid(std::max(1, mblocks), (K + 31) / 32);
+  long long launches = 0;
   for (int it = 0; it < iters; ++it) {
-    bnr_primal<<<blocks_for(nk), 256, 0, s>>>(nk, K, b->c, b->eta, b->omega, b->X, b->AtY,
-                                              b->L, b->U, b->Xn, b->dX);
+    // an empty side has no rows to step and no sums to write
+    if (nblocks > 0)
+      bnr_primal<<<ngrid, tb, 0, s>>>(b->n, K, mblocks, b->c, b->eta, b->omega, b->X, b->AtY,
+                                      b->L, b->U, b->Xn, b->dX, b->part);
     bnr_spmm<<<blocks_for(mk), 256, 0, s>>>(b->m, K, b->rp, b->ri, b->rx, b->dX, b->AdX);
-    bnr_dual<<<blocks_for(mk), 256, 0, s>>>(mk, K, b->rl, b->ru, b->eta, b->omega, b->Y, b->AX,
-                                            b->AdX, b->Yn, b->dY);
+    if (mblocks > 0)
+      bnr_dual<<<mgrid, tb, 0, s>>>(b->m, K, b->rl, b->ru, b->eta, b->omega, b->Y, b->AX,
+                                    b->AdX, b->Yn, b->dY, b->part);
     bnr_spmm<<<blocks_for(nk), 256, 0, s>>>(b->n, K, b->cp, b->ci, b->cx, b->dY, b->AtdY);
-    bnr_sums<<<sgrid, sblock, 0, s>>>(b->m, b->n, K, mblocks, b->dY, b->AdX, b->dX, b->part);
     bnr_accept<<<(K + 127) / 128, 128, 0, s>>>(K, mblocks, nblocks, b->part, b->eta, b->omega,
                                                b->accept, b->fac + 2 * it);
     bnr_update_n<<<blocks_for(nk), 256, 0, s>>>(nk, K, b->accept, b->X, b->Xn, b->AtY, b->AtdY);
     bnr_update_m<<<blocks_for(mk), 256, 0, s>>>(mk, K, b->accept, b->Y, b->Yn, b->AX, b->AdX);
+    launches += 5 + (nblocks > 0) + (mblocks > 0);
   }
+  return launches;
 }
 
 }  // namespace
@@ -498,7 +513,7 @@ int pdlp_bnr_solve_batch(pdlp_bnr* b, int32_t K, const double* col_lb, const dou
       PDLP_CUDA(cudaMalloc(&b->fac, sizeof(double) * fac.size()));
       PDLP_CUDA(cudaMemcpy(b->fac, fac.data(), sizeof(double) * fac.size(), cudaMemcpyHostToDevice));
       PDLP_CUDA(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
-      bnr_enqueue_iterations(b, K, iters, b->cap_stream);
+      b->g_launches = bnr_enqueue_iterations(b, K, iters, b->cap_stream);
       cudaGraph_t g = nullptr;
       const cudaError_t le = cudaGetLastError();
       const cudaError_t ce = cudaStreamEndCapture(b->cap_stream, &g);
@@ -510,7 +525,7 @@ int pdlp_bnr_solve_batch(pdlp_bnr* b, int32_t K, const double* col_lb, const dou
       b->g_k = K; b->g_iters = iters; b->g_growth = step_growth; b->g_damp = step_damp;
     }
     PDLP_CUDA(cudaGraphLaunch(b->graph, st));
-    count_launches(8LL * iters);
+    count_launches(b->g_launches);
   }
   // the bound: A^T Y, its terms, then per node (safebound.py:194-235)
   const int mblocks = (b->m + kRowsPerBlock - 1) / kRowsPerBlock;

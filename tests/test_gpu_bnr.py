@@ -98,7 +98,7 @@ def test_two_calls_match_oracle_bitwise(require_gpu, name):
         same(e.step_sizes(K)[0], o.eta[:K])
         # and the reference's own bounds, to the summation drift
         close(r.bounds, g[f"bounds{call}"])
-    assert e.Y is r2.y
+    assert e.Y is r.y
     st = e.stats()
     assert st["batches"] == 2 and st["nodes_bounded"] == 2 * K
     assert st["pdhg_iterations"] == 2 * int(g["iters"])
@@ -185,3 +185,32 @@ def test_arguments_are_checked(require_gpu):
     prob, sc = scaled_problem(g)
     with pytest.raises(ValueError):
         BNREngine(prob, sc, BNRConfig(device="cpu"))
+
+
+def test_ragged_node_tile_and_tiny_problem(require_gpu):
+    """K = 33 (one full 32-node tile and one node in the next) on a golden
+    problem, and a 1-row, 3-column LP, each bitwise the tree-order oracle."""
+    g = load("bnr_batch_s11")
+    rng = np.random.default_rng(33)
+    K = 33
+    cols = rng.integers(0, int(g["K"]), K)
+    L, U = g["L2"][:, cols], g["U2"][:, cols]
+    e, o = engine(g, batch=K, iters=20), oracle(g, batch=K, iters=20)
+    r, ro = e.solve_batch(L, U), o.solve_batch(L, U)
+    same(r.bounds, ro.bounds)
+    same(r.x, ro.x)
+    same(r.y, ro.y)
+
+    A = SparseMatrix.from_dense(np.array([[1.0, 2.0, -1.0]]))
+    prob = SimpleNamespace(A=A, c=np.array([1.0, -1.0, 0.5]), row_lb=np.array([1.0]),
+                           row_ub=np.array([1.0]), obj_offset=0.25)
+    L = np.zeros((3, 2))
+    U = np.array([[1.0, 1.0], [1.0, 0.5], [2.0, 2.0]])
+    e = BNREngine(prob, SimpleNamespace(obj=2.0), BNRConfig(batch=2, iters=40, device="gpu"))
+    o = BNROracle(A.rp, A.ri, A.rx, A.cp, A.ci, A.cx, prob.c, prob.row_lb, prob.row_ub, 2.0,
+                  0.25, batch=2, iters=40, sum_order="tree")
+    r, ro = e.solve_batch(L, U), o.solve_batch(L, U)
+    same(r.bounds, ro.bounds)
+    same(r.x, ro.x)
+    same(r.y, ro.y)
+    assert np.isfinite(r.bounds).all()

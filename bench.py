@@ -597,9 +597,10 @@ def run_spmv(args):
 def bnr_bytes_per_iteration(m, n, nnz, K):
     """Algorithmic HBM bytes of one batched PDHG iteration over K nodes: each
     (rows, K) float64 block read or written once per kernel that touches it
-    (primal 6 n-blocks, A dX 1 n + 1 m, dual 5 m, A^T dY 1 m + 1 n, sums 2 m +
-    1 n, updates 5 n + 5 m), plus the CSR and CSC matrices once each."""
-    return 8 * 14 * (m + n) * K + 2 * (12 * nnz + 8 * (max(m, n) + 1))
+    (primal with its sum: 6 n-blocks; A dX: 1 n + 1 m; dual with its sums:
+    5 m; A^T dY: 1 m + 1 n; updates: 5 n + 5 m), plus the CSR and CSC
+    matrices once each."""
+    return 8 * (13 * n + 12 * m) * K + 12 * nnz + 8 * (m + 1) + 12 * nnz + 8 * (n + 1)
 
 
 def run_bnr(args):

@@ -11,9 +11,10 @@ reference's CPU results bit for bit.  ``tests/golden/bnr/*.npz``, made by
 
 ``sum_order="tree"`` replaces the per-node sums over rows (the step-size
 test's three inner products and the two halves of the safe bound) by the
-device engine's fixed order -- blocks of 64 rows in order, each the sum of 8
-phases (rows ``b*64 + y + 8 j``, ``j`` ascending), phases added in order --
-and leaves every other operation as it is.  With it the oracle predicts the
+device engine's fixed order, and leaves every other operation as it is:
+blocks of 64 rows, each the sum of 8 phases (rows ``b*64 + y + 8 j``, ``j``
+ascending) added in phase order; then 32 lanes, lane ``l`` adding blocks
+``l, l + 32, ...`` in order; then the lanes in order.  With it the oracle predicts the
 device engine bit for bit; the default ``"sequential"`` is the reference's
 NumPy order.
 
@@ -40,10 +41,11 @@ def sum_rows(P):
 
 
 def sum_rows_tree(P, block=64, phases=8):
-    """The device engine's per-node sum over rows (``bnr_sums`` /
-    ``bnr_accept`` in csrc/bnr.cu): per block of 64 rows, phase ``y`` adds
-    rows ``y, y + 8, ...`` from 0.0; the phases are added in order; the
-    blocks are added in order from 0.0."""
+    """The device engine's per-node sum over rows (``bnr_block_sums`` and
+    ``warp_blocks_sum`` in csrc/bnr.cu): per block of 64 rows, phase ``y``
+    adds rows ``y, y + 8, ...`` from 0.0 and the phases are added in order;
+    lane ``l`` of 32 adds blocks ``l, l + 32, ...`` in order from 0.0; the
+    lane sums are added in lane order."""
     rows, K = P.shape
     nb = -(-rows // block)
     Q = np.zeros((nb * block, K))
@@ -55,9 +57,12 @@ def sum_rows_tree(P, block=64, phases=8):
     a = s[:, 0]
     for y in range(1, phases):
         a = a + s[:, y]
-    total = np.zeros(K)
+    lanes = np.zeros((32, K))
     for b in range(nb):
-        total = total + a[b]
+        lanes[b % 32] = lanes[b % 32] + a[b]
+    total = lanes[0]
+    for lane in range(1, 32):
+        total = total + lanes[lane]
     return total
 
 

@@ -47,32 +47,85 @@ __device__ __forceinline__ double clipd(double v, double lo, double hi) {
   return np_min(np_max(v, lo), hi);     // numpy.clip: maximum, then minimum
 }
 
-// Y (rows, k) = A X with X (cols, k) node-fastest; one thread per (row, node),
-// entries in storage order (the reference's CSR SpMM order).
+// Y (rows, k) = A X with X (cols, k) node-fastest.  One thread per (row, V
+// consecutive nodes): V = 2 when k is even (16-byte gathers and stores), else
+// 1.  Each node's entries are added in storage order (the reference's CSR
+// SpMM order).  The entries are taken eight at a time: their indices, values
+// and gathered X elements are all loaded before the adds, so a thread's
+// gathers are in flight together instead of one after another.
+template <int V>
+struct Lanes;
+template <>
+struct Lanes<1> {
+  double v[1];
+  __device__ static Lanes load(const double* p) { return Lanes{{*p}}; }
+  __device__ void store(double* p) const { *p = v[0]; }
+};
+template <>
+struct Lanes<2> {
+  double v[2];
+  __device__ static Lanes load(const double* p) {
+    const double2 t = *reinterpret_cast<const double2*>(p);
+    return Lanes{{t.x, t.y}};
+  }
+  __device__ void store(double* p) const { *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]); }
+};
+
+template <int V>
 __global__ void __launch_bounds__(256) bnr_spmm(int rows, int k, const int64_t* __restrict__ rp,
                                                 const int* __restrict__ ri,
                                                 const double* __restrict__ rx,
                                                 const double* __restrict__ X,
                                                 double* __restrict__ Y) {
+  constexpr int kBatch = 8;
+  const int groups = k / V;
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= (long long)rows * k) return;
-  const long long r = g / k;
-  const int col = (int)(g - r * k);
-  double acc = 0.0;
-  for (long long p = __ldg(rp + r); p < __ldg(rp + r + 1); ++p)
-    acc = add(acc, mul(__ldg(rx + p), X[(long long)__ldg(ri + p) * k + col]));
-  Y[g] = acc;
+  if (g >= (long long)rows * groups) return;
+  const long long r = g / groups;
+  const int col = (int)(g - r * groups) * V;
+  const double* Xc = X + col;
+  long long p = __ldg(rp + r);
+  const long long end = __ldg(rp + r + 1);
+  double acc[V];
+#pragma unroll
+  for (int u = 0; u < V; ++u) acc[u] = 0.0;
+  for (; p + kBatch <= end; p += kBatch) {
+    double v[kBatch];
+    Lanes<V> x[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      v[u] = __ldg(rx + p + u);
+      x[u] = Lanes<V>::load(Xc + (long long)__ldg(ri + p + u) * k);
+    }
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u)
+#pragma unroll
+      for (int e = 0; e < V; ++e) acc[e] = add(acc[e], mul(v[u], x[u].v[e]));
+  }
+  for (; p < end; ++p) {
+    const double v = __ldg(rx + p);
+    const Lanes<V> x = Lanes<V>::load(Xc + (long long)__ldg(ri + p) * k);
+#pragma unroll
+    for (int e = 0; e < V; ++e) acc[e] = add(acc[e], mul(v, x.v[e]));
+  }
+  Lanes<V> out;
+#pragma unroll
+  for (int e = 0; e < V; ++e) out.v[e] = acc[e];
+  out.store(Y + r * k + col);
 }
 
 // The per-node sums over rows run in a fixed order: blocks of kRowsPerBlock
 // rows; in a block, phase y (threadIdx.y, 8 phases) adds rows r0 + y + 8 j
-// for j ascending from 0.0; the phases are added in order; bnr_accept adds
-// the blocks in order.  The element-wise kernels below walk their rows in that
+// for j ascending from 0.0; the phases are added in order; then
+// warp_blocks_sum adds the blocks.  The element-wise kernels below walk their rows in that
 // layout, block (32, 8) with threadIdx.x the node within a 32-node tile, and
-// sum as they go.  Output pair of row block b and node j at part[2 (b k + j)]:
-// m-side blocks [0, mblocks), n-side blocks [mblocks, mblocks + nblocks).
+// sum as they go.  Output pair of row block b and node j at
+// part[2 (j pstride + b)], pstride = mblocks + nblocks + 1, so one node's
+// partials are contiguous for the warp that adds them: m-side blocks
+// [0, mblocks), n-side blocks [mblocks, mblocks + nblocks).
 __device__ __forceinline__ void bnr_block_sums(double s0, double s1, int k, int node,
-                                               long long part_block, double* __restrict__ part) {
+                                               int pstride, int part_block,
+                                               double* __restrict__ part) {
   __shared__ double sh[2][8][32];
   sh[0][threadIdx.y][threadIdx.x] = s0;
   sh[1][threadIdx.y][threadIdx.x] = s1;
@@ -83,7 +136,7 @@ __device__ __forceinline__ void bnr_block_sums(double s0, double s1, int k, int 
       a = add(a, sh[0][y][threadIdx.x]);
       c2 = add(c2, sh[1][y][threadIdx.x]);
     }
-    double* out = part + (part_block * k + node) * 2;
+    double* out = part + ((long long)node * pstride + part_block) * 2;
     out[0] = a;
     out[1] = c2;
   }
@@ -91,7 +144,7 @@ __device__ __forceinline__ void bnr_block_sums(double s0, double s1, int k, int 
 
 // Xn = clip(X - tau (c + AtY), L, U), dX = Xn - X (bnr.py:233-236), and the
 // node's sum of dX dX over the block's rows.
-__global__ void __launch_bounds__(256) bnr_primal(int n, int k, int mblocks,
+__global__ void __launch_bounds__(256) bnr_primal(int n, int k, int mblocks, int pstride,
                                                   const double* __restrict__ c,
                                                   const double* __restrict__ eta,
                                                   const double* __restrict__ omega,
@@ -116,12 +169,13 @@ __global__ void __launch_bounds__(256) bnr_primal(int n, int k, int mblocks,
       s = add(s, mul(d, d));
     }
   }
-  bnr_block_sums(s, 0.0, k, node, (long long)mblocks + blockIdx.x, part);
+  bnr_block_sums(s, 0.0, k, node, pstride, mblocks + blockIdx.x, part);
 }
 
 // W = Y + sigma (AX + 2 AdX); Yn = W - sigma clip(W / sigma, rl, ru); dY = Yn - Y
 // (bnr.py:238-242), and the node's sums of dY AdX and dY dY over the block's rows.
-__global__ void __launch_bounds__(256) bnr_dual(int m, int k, const double* __restrict__ rl,
+__global__ void __launch_bounds__(256) bnr_dual(int m, int k, int pstride,
+                                                const double* __restrict__ rl,
                                                 const double* __restrict__ ru,
                                                 const double* __restrict__ eta,
                                                 const double* __restrict__ omega,
@@ -147,25 +201,42 @@ __global__ void __launch_bounds__(256) bnr_dual(int m, int k, const double* __re
       s1 = add(s1, mul(d, d));
     }
   }
-  bnr_block_sums(s0, s1, k, node, blockIdx.x, part);
+  bnr_block_sums(s0, s1, k, node, pstride, blockIdx.x, part);
 }
 
-// Per node: the sums in block order, then the step test and the next step size
-// (bnr.py:244-270).  accept[node] is 1 when the trial is taken.  fac holds the
-// iteration's (1 - t^-growth, 1 + t^-damp), computed on the host with the C
-// library's pow, as the reference computes them.
-__global__ void bnr_accept(int k, int mblocks, int nblocks, const double* __restrict__ part,
-                           double* __restrict__ eta, const double* __restrict__ omega,
-                           int* __restrict__ accept, const double* __restrict__ fac) {
-  const int node = blockIdx.x * blockDim.x + threadIdx.x;
-  if (node >= k) return;
-  double dyadx = 0.0, dydy = 0.0, dxdx = 0.0;
-  for (int b = 0; b < mblocks; ++b) {
-    const double* p = part + ((long long)b * k + node) * 2;
-    dyadx = add(dyadx, p[0]);
-    dydy = add(dydy, p[1]);
-  }
-  for (int b = 0; b < nblocks; ++b) dxdx = add(dxdx, part[((long long)(mblocks + b) * k + node) * 2]);
+// The sum over nb row blocks (from block b0) of slot c of a node's partials,
+// by one warp: lane l adds blocks l, l + 32, ... in order from 0.0, then the
+// 32 lane sums are added in lane order.  Every lane returns the total.
+__device__ __forceinline__ double warp_blocks_sum(const double* __restrict__ part, int pstride,
+                                                  int node, int b0, int nb, int c, int lane) {
+  const double* p = part + ((long long)node * pstride + b0) * 2 + c;
+  double s = 0.0;
+#pragma unroll 4
+  for (int b = lane; b < nb; b += 32) s = add(s, p[2 * b]);
+  double a = __shfl_sync(0xffffffffu, s, 0);
+  for (int l = 1; l < 32; ++l) a = add(a, __shfl_sync(0xffffffffu, s, l));
+  return a;
+}
+
+// Per node (one warp each): the step-size test's sums over the row blocks,
+// then the test and the next step size (bnr.py:244-270).  accept[node] is 1
+// when the trial is taken.  fac holds the iteration's (1 - t^-growth,
+// 1 + t^-damp), computed on the host with the C library's pow, as the
+// reference computes them.
+__global__ void __launch_bounds__(128) bnr_accept(int k, int mblocks, int nblocks,
+                                                  const double* __restrict__ part,
+                                                  double* __restrict__ eta,
+                                                  const double* __restrict__ omega,
+                                                  int* __restrict__ accept,
+                                                  const double* __restrict__ fac) {
+  const int lane = threadIdx.x & 31;
+  const int node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (node >= k) return;            // whole warps leave together
+  const int pstride = mblocks + nblocks + 1;
+  const double dyadx = warp_blocks_sum(part, pstride, node, 0, mblocks, 0, lane);
+  const double dydy = warp_blocks_sum(part, pstride, node, 0, mblocks, 1, lane);
+  const double dxdx = warp_blocks_sum(part, pstride, node, mblocks, nblocks, 0, lane);
+  if (lane != 0) return;
   const double om = omega[node];
   const double interaction = fabs(dyadx);
   const double movement = mul(0.5, add(mul(om, dxdx), dydy / om));
@@ -211,10 +282,11 @@ __global__ void bnr_clip(long long total, double* __restrict__ X, const double* 
 
 // Safe dual bound terms (safebound.py:212-230), per-node partial sums and
 // flags over blocks of rows: the m side from Y, the n side from d = c - A^T Y.
-// part[block][node] = (sum, flags): flag 1 = a vacuous term, flag 2 = an empty
-// column box L > U + 1e-12 (bnr.py:203).
+// The pair of (node, block), laid out as for the step sums, is (sum, flags):
+// flag 1 = a vacuous term, flag 2 = an empty column box L > U + 1e-12
+// (bnr.py:203).
 __global__ void __launch_bounds__(256) bnr_bound_terms(
-    int m, int n, int k, int mblocks, const double* __restrict__ Y,
+    int m, int n, int k, int mblocks, int pstride, const double* __restrict__ Y,
     const double* __restrict__ rl, const double* __restrict__ ru,
     const double* __restrict__ c, const double* __restrict__ aty,
     const double* __restrict__ L, const double* __restrict__ U, double* __restrict__ part) {
@@ -258,7 +330,7 @@ __global__ void __launch_bounds__(256) bnr_bound_terms(
       a = add(a, sh[yy][threadIdx.x]);
       f |= bad_sh[yy][threadIdx.x];
     }
-    double* out = part + ((long long)blockIdx.x * k + node) * 2;
+    double* out = part + ((long long)node * pstride + blockIdx.x) * 2;
     out[0] = a;
     out[1] = (double)f;
   }
@@ -266,24 +338,22 @@ __global__ void __launch_bounds__(256) bnr_bound_terms(
 
 // Per node: bound = (row sum + column sum + offset) / obj_scale, -inf when
 // vacuous, +inf for an empty box; also the infeasible flag (bnr.py:203, 283-290).
-__global__ void bnr_bound_final(int k, int mblocks, int nblocks,
-                                const double* __restrict__ part, double obj_offset,
-                                double obj_scale, double* __restrict__ bounds,
-                                unsigned char* __restrict__ empty) {
-  const int node = blockIdx.x * blockDim.x + threadIdx.x;
-  if (node >= k) return;
-  double rs = 0.0, cs = 0.0;
+__global__ void __launch_bounds__(128) bnr_bound_final(int k, int mblocks, int nblocks,
+                                                       const double* __restrict__ part,
+                                                       double obj_offset, double obj_scale,
+                                                       double* __restrict__ bounds,
+                                                       unsigned char* __restrict__ empty) {
+  const int lane = threadIdx.x & 31;
+  const int node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (node >= k) return;            // whole warps leave together
+  const int pstride = mblocks + nblocks + 1;
+  const double rs = warp_blocks_sum(part, pstride, node, 0, mblocks, 0, lane);
+  const double cs = warp_blocks_sum(part, pstride, node, mblocks, nblocks, 0, lane);
   int flags = 0;
-  for (int b = 0; b < mblocks; ++b) {
-    const double* p = part + ((long long)b * k + node) * 2;
-    rs = add(rs, p[0]);
-    flags |= (int)p[1];
-  }
-  for (int b = 0; b < nblocks; ++b) {
-    const double* p = part + ((long long)(mblocks + b) * k + node) * 2;
-    cs = add(cs, p[0]);
-    flags |= (int)p[1];
-  }
+  for (int b = lane; b < mblocks + nblocks; b += 32)
+    flags |= (int)part[((long long)node * pstride + b) * 2 + 1];
+  flags = __reduce_or_sync(0xffffffffu, flags);
+  if (lane != 0) return;
   const bool vac = flags & 1, emp = flags & 2;
   const double bound = vac ? -INFINITY : add(rs, cs);
   bounds[node] = emp ? INFINITY : (bound + obj_offset) / obj_scale;
@@ -291,6 +361,15 @@ __global__ void bnr_bound_final(int k, int mblocks, int nblocks,
 }
 
 int blocks_for(long long total) { return (int)std::max(1LL, (total + 255) / 256); }
+
+// Y (rows, k) = A X on stream s, two nodes per thread when k is even.
+void launch_spmm(int rows, int k, const int64_t* rp, const int* ri, const double* rx,
+                 const double* X, double* Y, cudaStream_t s) {
+  if (k % 2 == 0)
+    bnr_spmm<2><<<blocks_for((long long)rows * (k / 2)), 256, 0, s>>>(rows, k, rp, ri, rx, X, Y);
+  else
+    bnr_spmm<1><<<blocks_for((long long)rows * k), 256, 0, s>>>(rows, k, rp, ri, rx, X, Y);
+}
 
 }  // namespace
 }  // namespace pdlp
@@ -390,15 +469,15 @@ long long bnr_enqueue_iterations(pdlp_bnr* b, int K, int iters, cudaStream_t s) 
   for (int it = 0; it < iters; ++it) {
     // an empty side has no rows to step and no sums to write
     if (nblocks > 0)
-      bnr_primal<<<ngrid, tb, 0, s>>>(b->n, K, mblocks, b->c, b->eta, b->omega, b->X, b->AtY,
+      bnr_primal<<<ngrid, tb, 0, s>>>(b->n, K, mblocks, mblocks + nblocks + 1, b->c, b->eta, b->omega, b->X, b->AtY,
                                       b->L, b->U, b->Xn, b->dX, b->part);
-    bnr_spmm<<<blocks_for(mk), 256, 0, s>>>(b->m, K, b->rp, b->ri, b->rx, b->dX, b->AdX);
+    launch_spmm(b->m, K, b->rp, b->ri, b->rx, b->dX, b->AdX, s);
     if (mblocks > 0)
-      bnr_dual<<<mgrid, tb, 0, s>>>(b->m, K, b->rl, b->ru, b->eta, b->omega, b->Y, b->AX,
+      bnr_dual<<<mgrid, tb, 0, s>>>(b->m, K, mblocks + nblocks + 1, b->rl, b->ru, b->eta, b->omega, b->Y, b->AX,
                                     b->AdX, b->Yn, b->dY, b->part);
-    bnr_spmm<<<blocks_for(nk), 256, 0, s>>>(b->n, K, b->cp, b->ci, b->cx, b->dY, b->AtdY);
-    bnr_accept<<<(K + 127) / 128, 128, 0, s>>>(K, mblocks, nblocks, b->part, b->eta, b->omega,
-                                               b->accept, b->fac + 2 * it);
+    launch_spmm(b->n, K, b->cp, b->ci, b->cx, b->dY, b->AtdY, s);
+    bnr_accept<<<(K + 3) / 4, 128, 0, s>>>(K, mblocks, nblocks, b->part, b->eta, b->omega,
+                                           b->accept, b->fac + 2 * it);
     bnr_update_n<<<blocks_for(nk), 256, 0, s>>>(nk, K, b->accept, b->X, b->Xn, b->AtY, b->AtdY);
     bnr_update_m<<<blocks_for(mk), 256, 0, s>>>(mk, K, b->accept, b->Y, b->Yn, b->AX, b->AdX);
     launches += 5 + (nblocks > 0) + (mblocks > 0);
@@ -490,8 +569,8 @@ int pdlp_bnr_solve_batch(pdlp_bnr* b, int32_t K, const double* col_lb, const dou
   PDLP_CUDA(cudaMemcpyAsync(b->omega, b->h_omega.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
   // X = clip(X, L, U); AX = A X; AtY = A^T Y
   bnr_clip<<<blocks_for((long long)nk), 256, 0, st>>>((long long)nk, b->X, b->L, b->U);
-  bnr_spmm<<<blocks_for((long long)mk), 256, 0, st>>>(b->m, K, b->rp, b->ri, b->rx, b->X, b->AX);
-  bnr_spmm<<<blocks_for((long long)nk), 256, 0, st>>>(b->n, K, b->cp, b->ci, b->cx, b->Y, b->AtY);
+  launch_spmm(b->m, K, b->rp, b->ri, b->rx, b->X, b->AX, st);
+  launch_spmm(b->n, K, b->cp, b->ci, b->cx, b->Y, b->AtY, st);
   count_launches(3);
   PDLP_CUDA(cudaGetLastError());
   // the iterations, from a graph captured once per (K, iters, exponents)
@@ -530,11 +609,12 @@ int pdlp_bnr_solve_batch(pdlp_bnr* b, int32_t K, const double* col_lb, const dou
   // the bound: A^T Y, its terms, then per node (safebound.py:194-235)
   const int mblocks = (b->m + kRowsPerBlock - 1) / kRowsPerBlock;
   const int nblocks = (b->n + kRowsPerBlock - 1) / kRowsPerBlock;
-  bnr_spmm<<<blocks_for((long long)nk), 256, 0, st>>>(b->n, K, b->cp, b->ci, b->cx, b->Y, b->AtdY);
+  launch_spmm(b->n, K, b->cp, b->ci, b->cx, b->Y, b->AtdY, st);
   bnr_bound_terms<<<dim3(std::max(1, mblocks + nblocks), (K + 31) / 32), dim3(32, 8), 0, st>>>(
-      b->m, b->n, K, mblocks, b->Y, b->rl, b->ru, b->c, b->AtdY, b->L, b->U, b->part);
-  bnr_bound_final<<<(K + 127) / 128, 128, 0, st>>>(K, mblocks, nblocks, b->part, b->obj_offset,
-                                                   b->obj_scale, b->bounds, b->empty);
+      b->m, b->n, K, mblocks, mblocks + nblocks + 1, b->Y, b->rl, b->ru, b->c, b->AtdY, b->L, b->U,
+      b->part);
+  bnr_bound_final<<<(K + 3) / 4, 128, 0, st>>>(K, mblocks, nblocks, b->part, b->obj_offset,
+                                               b->obj_scale, b->bounds, b->empty);
   count_launches(3);
   PDLP_CUDA(cudaGetLastError());
   // outputs; the step sizes stay with the engine for the next call

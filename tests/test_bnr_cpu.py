@@ -77,12 +77,12 @@ def test_tree_order_drift_from_reference_is_bounded(name):
     assert rel(o.eta[:K], g["eta2"]) <= 1e-5
 
 
-def test_tree_sum_is_the_block_phase_order():
+def test_tree_sum_is_the_block_phase_lane_order():
     from oracle.bnr_oracle import sum_rows_tree
     rng = np.random.default_rng(1)
-    for rows in (1, 7, 64, 65, 230):
+    for rows in (1, 7, 64, 65, 230, 64 * 40 + 3):
         P = rng.standard_normal((rows, 3))
-        want = np.zeros(3)
+        blocks = []
         for b0 in range(0, rows, 64):
             blk = P[b0:b0 + 64]
             ph = [np.zeros(3) for _ in range(8)]
@@ -91,7 +91,13 @@ def test_tree_sum_is_the_block_phase_order():
             a = ph[0]
             for y in range(1, 8):
                 a = a + ph[y]
-            want = want + a
+            blocks.append(a)
+        lanes = [np.zeros(3) for _ in range(32)]
+        for b, a in enumerate(blocks):
+            lanes[b % 32] = lanes[b % 32] + a
+        want = lanes[0]
+        for lane in range(1, 32):
+            want = want + lanes[lane]
         assert np.array_equal(sum_rows_tree(P), want)
 
 

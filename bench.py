@@ -595,12 +595,13 @@ def run_spmv(args):
 
 
 def bnr_bytes_per_iteration(m, n, nnz, K):
-    """Algorithmic HBM bytes of one batched PDHG iteration over K nodes: each
-    (rows, K) float64 block read or written once per kernel that touches it
-    (primal with its sum: 6 n-blocks; A dX: 1 n + 1 m; dual with its sums:
-    5 m; A^T dY: 1 m + 1 n; updates: 5 n + 5 m), plus the CSR and CSC
-    matrices once each."""
-    return 8 * (13 * n + 12 * m) * K + 12 * nnz + 8 * (m + 1) + 12 * nnz + 8 * (n + 1)
+    """Algorithmic HBM bytes of one batched PDHG iteration over K nodes, every
+    trial taken: each (rows, K) float64 block read or written once per kernel
+    that touches it -- primal step with its sum (reads X, AtY, AtdY, L, U;
+    writes X, AtY, dX: 8 n-blocks), A dX (1 n + 1 m), dual step with its
+    sums (reads Y, AX, both A dX; writes Y, AX, dY: 7 m), A^T dY (1 m + 1 n)
+    -- plus the CSR and CSC matrices once each."""
+    return 8 * (10 * n + 9 * m) * K + 12 * nnz + 8 * (m + 1) + 12 * nnz + 8 * (n + 1)
 
 
 def run_bnr(args):

@@ -7,9 +7,11 @@
 //
 // Layout: every per-node block is (rows, K) with the node index fastest, so a
 // sparse product reads A once for all K nodes (A X with X (n, K)).  One
-// iteration is seven launches:
+// iteration is five launches:
 //   primal step (+ sum dX dX)  ->  A dX  ->  dual step (+ sums dY AdX, dY dY)
-//   ->  A^T dY  ->  per-node accept / step size  ->  n-side and m-side updates.
+//   ->  A^T dY  ->  per-node accept / step size.
+// A taken trial is not stored but redone by the next step, which reads the
+// same inputs anyway (see bnr_primal).
 // The iterations of one call are captured once into a CUDA graph, keyed by
 // (K, iterations, step exponents), and replayed.
 //
@@ -72,7 +74,7 @@ struct Lanes<2> {
 };
 
 template <int V>
-__global__ void __launch_bounds__(256) bnr_spmm(int rows, int k, const int64_t* __restrict__ rp,
+__global__ void __launch_bounds__(256, 1) bnr_spmm(int rows, int k, const int64_t* __restrict__ rp,
                                                 const int* __restrict__ ri,
                                                 const double* __restrict__ rx,
                                                 const double* __restrict__ X,
@@ -142,29 +144,49 @@ __device__ __forceinline__ void bnr_block_sums(double s0, double s1, int k, int 
   }
 }
 
+// A taken trial is not stored: the next step recomputes it.  pend[j] says
+// that node j's last trial was taken, and eta_prev[j] is the step size that
+// trial used.  The next primal and dual steps read X, AtY, Y and AX anyway;
+// for a pending node they first redo the trial from them with the same
+// operations, which gives the same bits, and store it as the current
+// iterate together with the reference's other updates on acceptance,
+// AtY += AtdY and AX += AdX (bnr.py:262-265).  Nothing is copied, and one
+// buffer per iterate suffices.
+
 // Xn = clip(X - tau (c + AtY), L, U), dX = Xn - X (bnr.py:233-236), and the
 // node's sum of dX dX over the block's rows.
 __global__ void __launch_bounds__(256) bnr_primal(int n, int k, int mblocks, int pstride,
                                                   const double* __restrict__ c,
                                                   const double* __restrict__ eta,
+                                                  const double* __restrict__ eta_prev,
                                                   const double* __restrict__ omega,
-                                                  const double* __restrict__ X,
-                                                  const double* __restrict__ AtY,
+                                                  const int* __restrict__ pend,
+                                                  double* __restrict__ X,
+                                                  double* __restrict__ AtY,
+                                                  const double* __restrict__ AtdY,
                                                   const double* __restrict__ L,
                                                   const double* __restrict__ U,
-                                                  double* __restrict__ Xn, double* __restrict__ dX,
+                                                  double* __restrict__ dX,
                                                   double* __restrict__ part) {
   const int node = blockIdx.y * 32 + threadIdx.x;
   double s = 0.0;
   if (node < k) {
     const double tau = eta[node] / omega[node];
+    const bool taken = pend[node] != 0;
+    const double tau_prev = eta_prev[node] / omega[node];
     const int r0 = blockIdx.x * kRowsPerBlock, r1 = min(n, r0 + kRowsPerBlock);
     for (int r = r0 + threadIdx.y; r < r1; r += 8) {
       const long long g = (long long)r * k + node;
-      const double x = X[g];
-      const double xn = clipd(sub(x, mul(tau, add(__ldg(c + r), AtY[g]))), L[g], U[g]);
+      const double cr = __ldg(c + r), lo = L[g], hi = U[g];
+      double x = X[g], aty = AtY[g];
+      if (taken) {
+        x = clipd(sub(x, mul(tau_prev, add(cr, aty))), lo, hi);
+        aty = add(aty, AtdY[g]);
+        X[g] = x;
+        AtY[g] = aty;
+      }
+      const double xn = clipd(sub(x, mul(tau, add(cr, aty))), lo, hi);
       const double d = sub(xn, x);
-      Xn[g] = xn;
       dX[g] = d;
       s = add(s, mul(d, d));
     }
@@ -172,30 +194,47 @@ __global__ void __launch_bounds__(256) bnr_primal(int n, int k, int mblocks, int
   bnr_block_sums(s, 0.0, k, node, pstride, mblocks + blockIdx.x, part);
 }
 
+// The dual trial of a node with step sigma (bnr.py:238-242).
+__device__ __forceinline__ double dual_trial(double y, double ax, double adx, double sigma,
+                                             double lo, double hi) {
+  const double w = add(y, mul(sigma, add(ax, mul(2.0, adx))));
+  return sub(w, mul(sigma, clipd(w / sigma, lo, hi)));
+}
+
 // W = Y + sigma (AX + 2 AdX); Yn = W - sigma clip(W / sigma, rl, ru); dY = Yn - Y
-// (bnr.py:238-242), and the node's sums of dY AdX and dY dY over the block's rows.
+// (bnr.py:238-242), and the node's sums of dY AdX and dY dY over the block's
+// rows.  AdX_prev is the previous step's A dX, which the redone trial uses.
 __global__ void __launch_bounds__(256) bnr_dual(int m, int k, int pstride,
                                                 const double* __restrict__ rl,
                                                 const double* __restrict__ ru,
                                                 const double* __restrict__ eta,
+                                                const double* __restrict__ eta_prev,
                                                 const double* __restrict__ omega,
-                                                const double* __restrict__ Y,
-                                                const double* __restrict__ AX,
+                                                const int* __restrict__ pend,
+                                                double* __restrict__ Y, double* __restrict__ AX,
+                                                const double* __restrict__ AdX_prev,
                                                 const double* __restrict__ AdX,
-                                                double* __restrict__ Yn, double* __restrict__ dY,
+                                                double* __restrict__ dY,
                                                 double* __restrict__ part) {
   const int node = blockIdx.y * 32 + threadIdx.x;
   double s0 = 0.0, s1 = 0.0;
   if (node < k) {
     const double sigma = eta[node] * omega[node];
+    const bool taken = pend[node] != 0;
+    const double sigma_prev = eta_prev[node] * omega[node];
     const int r0 = blockIdx.x * kRowsPerBlock, r1 = min(m, r0 + kRowsPerBlock);
     for (int r = r0 + threadIdx.y; r < r1; r += 8) {
       const long long g = (long long)r * k + node;
-      const double y = Y[g], adx = AdX[g];
-      const double w = add(y, mul(sigma, add(AX[g], mul(2.0, adx))));
-      const double yn = sub(w, mul(sigma, clipd(w / sigma, __ldg(rl + r), __ldg(ru + r))));
-      const double d = sub(yn, y);
-      Yn[g] = yn;
+      const double lo = __ldg(rl + r), hi = __ldg(ru + r), adx = AdX[g];
+      double y = Y[g], ax = AX[g];
+      if (taken) {
+        const double adx_prev = AdX_prev[g];
+        y = dual_trial(y, ax, adx_prev, sigma_prev, lo, hi);
+        ax = add(ax, adx_prev);
+        Y[g] = y;
+        AX[g] = ax;
+      }
+      const double d = sub(dual_trial(y, ax, adx, sigma, lo, hi), y);
       dY[g] = d;
       s0 = add(s0, mul(d, adx));
       s1 = add(s1, mul(d, d));
@@ -219,13 +258,14 @@ __device__ __forceinline__ double warp_blocks_sum(const double* __restrict__ par
 }
 
 // Per node (one warp each): the step-size test's sums over the row blocks,
-// then the test and the next step size (bnr.py:244-270).  accept[node] is 1
-// when the trial is taken.  fac holds the iteration's (1 - t^-growth,
+// then the test and the next step size (bnr.py:244-270).  A taken trial sets
+// accept[node] (the next step's pend); eta_prev keeps the step it used.  fac holds the iteration's (1 - t^-growth,
 // 1 + t^-damp), computed on the host with the C library's pow, as the
 // reference computes them.
 __global__ void __launch_bounds__(128) bnr_accept(int k, int mblocks, int nblocks,
                                                   const double* __restrict__ part,
                                                   double* __restrict__ eta,
+                                                  double* __restrict__ eta_prev,
                                                   const double* __restrict__ omega,
                                                   int* __restrict__ accept,
                                                   const double* __restrict__ fac) {
@@ -244,33 +284,46 @@ __global__ void __launch_bounds__(128) bnr_accept(int k, int mblocks, int nblock
   const double limit = interaction > 0.0 ? movement / np_max(interaction, floor_) : INFINITY;
   const double e = eta[node];
   accept[node] = (e <= limit) || (movement == 0.0);
+  eta_prev[node] = e;
   double en = np_min(mul(fac[0], limit), mul(fac[1], e));
   en = fmax(isfinite(en) ? en : 1.0, 1e-14);
   eta[node] = en;
 }
 
-// n side: X = accept ? Xn : X, AtY = accept ? AtY + AtdY : AtY (bnr.py:262-265)
-__global__ void bnr_update_n(long long total, int k, const int* __restrict__ accept,
-                             double* __restrict__ X, const double* __restrict__ Xn,
-                             double* __restrict__ AtY, const double* __restrict__ AtdY) {
+// Each node's final iterates: for a node whose last trial was taken, that
+// trial, redone as in bnr_primal / bnr_dual; otherwise X and Y as they are.
+__global__ void bnr_resolve_x(long long total, int k, const int* __restrict__ pend,
+                              const double* __restrict__ eta_prev,
+                              const double* __restrict__ omega, const double* __restrict__ c,
+                              const double* __restrict__ X, const double* __restrict__ AtY,
+                              const double* __restrict__ L, const double* __restrict__ U,
+                              double* __restrict__ out) {
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= total) return;
-  if (accept[g % k]) {
-    X[g] = Xn[g];
-    AtY[g] = add(AtY[g], AtdY[g]);
+  const int node = (int)(g % k);
+  double x = X[g];
+  if (pend[node]) {
+    const double tau = eta_prev[node] / omega[node];
+    x = clipd(sub(x, mul(tau, add(c[g / k], AtY[g]))), L[g], U[g]);
   }
+  out[g] = x;
 }
 
-// m side: Y = accept ? Yn : Y, AX = accept ? AX + AdX : AX
-__global__ void bnr_update_m(long long total, int k, const int* __restrict__ accept,
-                             double* __restrict__ Y, const double* __restrict__ Yn,
-                             double* __restrict__ AX, const double* __restrict__ AdX) {
+__global__ void bnr_resolve_y(long long total, int k, const int* __restrict__ pend,
+                              const double* __restrict__ eta_prev,
+                              const double* __restrict__ omega, const double* __restrict__ rl,
+                              const double* __restrict__ ru, const double* __restrict__ Y,
+                              const double* __restrict__ AX, const double* __restrict__ AdX,
+                              double* __restrict__ out) {
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= total) return;
-  if (accept[g % k]) {
-    Y[g] = Yn[g];
-    AX[g] = add(AX[g], AdX[g]);
+  const int node = (int)(g % k);
+  double y = Y[g];
+  if (pend[node]) {
+    const long long i = g / k;
+    y = dual_trial(y, AX[g], AdX[g], eta_prev[node] * omega[node], rl[i], ru[i]);
   }
+  out[g] = y;
 }
 
 // X = clip(X, L, U) (bnr.py:211)
@@ -387,10 +440,13 @@ struct pdlp_bnr {
   double *rx = nullptr, *cx = nullptr, *c = nullptr, *rl = nullptr, *ru = nullptr;
   // per-node blocks, sized for cap nodes
   int cap = 0;
-  double *L = nullptr, *U = nullptr, *X = nullptr, *Xn = nullptr, *dX = nullptr, *AtY = nullptr,
+  // A dX in two buffers, alternating by iteration (a step redoes the
+  // previous trial with the previous A dX)
+  double *L = nullptr, *U = nullptr, *X = nullptr, *dX = nullptr, *AtY = nullptr,
          *AtdY = nullptr;
-  double *Y = nullptr, *Yn = nullptr, *dY = nullptr, *AX = nullptr, *AdX = nullptr;
-  double *eta = nullptr, *omega = nullptr, *part = nullptr, *bounds = nullptr;
+  double *Y = nullptr, *dY = nullptr, *AX = nullptr, *AdX0 = nullptr, *AdX1 = nullptr;
+  double *eta = nullptr, *eta_prev = nullptr, *omega = nullptr, *part = nullptr,
+         *bounds = nullptr;
   int* accept = nullptr;
   unsigned char* empty = nullptr;
   std::vector<double> h_eta, h_omega;   // persistent step sizes (bnr.py:168-171)
@@ -406,8 +462,8 @@ struct pdlp_bnr {
 namespace {
 
 void bnr_free_blocks(pdlp_bnr* b) {
-  double** ds[] = {&b->L, &b->U, &b->X, &b->Xn, &b->dX, &b->AtY, &b->AtdY, &b->Y, &b->Yn, &b->dY,
-                   &b->AX, &b->AdX, &b->eta, &b->omega, &b->part, &b->bounds};
+  double** ds[] = {&b->L, &b->U, &b->X, &b->dX, &b->AtY, &b->AtdY, &b->Y, &b->dY, &b->AX,
+                   &b->AdX0, &b->AdX1, &b->eta, &b->eta_prev, &b->omega, &b->part, &b->bounds};
   for (double** d : ds) { cudaFree(*d); *d = nullptr; }
   cudaFree(b->accept); b->accept = nullptr;
   cudaFree(b->empty); b->empty = nullptr;
@@ -424,9 +480,9 @@ int bnr_ensure(pdlp_bnr* b, int K) {
   const int mblocks = (b->m + kRowsPerBlock - 1) / kRowsPerBlock;
   const int nblocks = (b->n + kRowsPerBlock - 1) / kRowsPerBlock;
   struct { double** p; size_t n; } want[] = {
-      {&b->L, nk}, {&b->U, nk}, {&b->X, nk}, {&b->Xn, nk}, {&b->dX, nk}, {&b->AtY, nk},
-      {&b->AtdY, nk}, {&b->Y, mk}, {&b->Yn, mk}, {&b->dY, mk}, {&b->AX, mk}, {&b->AdX, mk},
-      {&b->eta, (size_t)cap}, {&b->omega, (size_t)cap},
+      {&b->L, nk}, {&b->U, nk}, {&b->X, nk}, {&b->dX, nk}, {&b->AtY, nk}, {&b->AtdY, nk},
+      {&b->Y, mk}, {&b->dY, mk}, {&b->AX, mk}, {&b->AdX0, mk}, {&b->AdX1, mk},
+      {&b->eta, (size_t)cap}, {&b->eta_prev, (size_t)cap}, {&b->omega, (size_t)cap},
       {&b->part, (size_t)(mblocks + nblocks + 1) * cap * 2}, {&b->bounds, (size_t)cap}};
   for (auto& w : want) {
     const cudaError_t e = cudaMalloc(w.p, sizeof(double) * std::max<size_t>(w.n, 1));
@@ -460,27 +516,28 @@ int bnr_upload(T** dst, const T* src, size_t count, int memory, cudaStream_t st)
 // The launches of `iters` iterations for K nodes, on stream s; returns how
 // many kernels it launched.
 long long bnr_enqueue_iterations(pdlp_bnr* b, int K, int iters, cudaStream_t s) {
-  const long long nk = (long long)b->n * K, mk = (long long)b->m * K;
   const int mblocks = (b->m + kRowsPerBlock - 1) / kRowsPerBlock;
   const int nblocks = (b->n + kRowsPerBlock - 1) / kRowsPerBlock;
   const dim3 tb(32, 8);
   const dim3 ngrid(std::max(1, nblocks), (K + 31) / 32), mgrid(std::max(1, mblocks), (K + 31) / 32);
   long long launches = 0;
   for (int it = 0; it < iters; ++it) {
+    double* adx = (it & 1) ? b->AdX1 : b->AdX0;        // this step's A dX
+    double* adx_prev = (it & 1) ? b->AdX0 : b->AdX1;   // the previous step's
     // an empty side has no rows to step and no sums to write
     if (nblocks > 0)
-      bnr_primal<<<ngrid, tb, 0, s>>>(b->n, K, mblocks, mblocks + nblocks + 1, b->c, b->eta, b->omega, b->X, b->AtY,
-                                      b->L, b->U, b->Xn, b->dX, b->part);
-    launch_spmm(b->m, K, b->rp, b->ri, b->rx, b->dX, b->AdX, s);
+      bnr_primal<<<ngrid, tb, 0, s>>>(b->n, K, mblocks, mblocks + nblocks + 1, b->c, b->eta,
+                                      b->eta_prev, b->omega, b->accept, b->X, b->AtY, b->AtdY,
+                                      b->L, b->U, b->dX, b->part);
+    launch_spmm(b->m, K, b->rp, b->ri, b->rx, b->dX, adx, s);
     if (mblocks > 0)
-      bnr_dual<<<mgrid, tb, 0, s>>>(b->m, K, mblocks + nblocks + 1, b->rl, b->ru, b->eta, b->omega, b->Y, b->AX,
-                                    b->AdX, b->Yn, b->dY, b->part);
+      bnr_dual<<<mgrid, tb, 0, s>>>(b->m, K, mblocks + nblocks + 1, b->rl, b->ru, b->eta,
+                                    b->eta_prev, b->omega, b->accept, b->Y, b->AX, adx_prev, adx,
+                                    b->dY, b->part);
     launch_spmm(b->n, K, b->cp, b->ci, b->cx, b->dY, b->AtdY, s);
-    bnr_accept<<<(K + 3) / 4, 128, 0, s>>>(K, mblocks, nblocks, b->part, b->eta, b->omega,
-                                           b->accept, b->fac + 2 * it);
-    bnr_update_n<<<blocks_for(nk), 256, 0, s>>>(nk, K, b->accept, b->X, b->Xn, b->AtY, b->AtdY);
-    bnr_update_m<<<blocks_for(mk), 256, 0, s>>>(mk, K, b->accept, b->Y, b->Yn, b->AX, b->AdX);
-    launches += 5 + (nblocks > 0) + (mblocks > 0);
+    bnr_accept<<<(K + 3) / 4, 128, 0, s>>>(K, mblocks, nblocks, b->part, b->eta, b->eta_prev,
+                                           b->omega, b->accept, b->fac + 2 * it);
+    launches += 3 + (nblocks > 0) + (mblocks > 0);
   }
   return launches;
 }
@@ -565,8 +622,11 @@ int pdlp_bnr_solve_batch(pdlp_bnr* b, int32_t K, const double* col_lb, const dou
     if (nk) PDLP_CUDA(cudaMemsetAsync(b->X, 0, sizeof(double) * nk, st));
     if (mk) PDLP_CUDA(cudaMemsetAsync(b->Y, 0, sizeof(double) * mk, st));
   }
+  // no trial pending at the start
+  PDLP_CUDA(cudaMemsetAsync(b->accept, 0, sizeof(int) * K, st));
   PDLP_CUDA(cudaMemcpyAsync(b->eta, b->h_eta.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
   PDLP_CUDA(cudaMemcpyAsync(b->omega, b->h_omega.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
+  PDLP_CUDA(cudaMemcpyAsync(b->eta_prev, b->h_eta.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
   // X = clip(X, L, U); AX = A X; AtY = A^T Y
   bnr_clip<<<blocks_for((long long)nk), 256, 0, st>>>((long long)nk, b->X, b->L, b->U);
   launch_spmm(b->m, K, b->rp, b->ri, b->rx, b->X, b->AX, st);
@@ -606,21 +666,28 @@ int pdlp_bnr_solve_batch(pdlp_bnr* b, int32_t K, const double* col_lb, const dou
     PDLP_CUDA(cudaGraphLaunch(b->graph, st));
     count_launches(b->g_launches);
   }
+  // each node's final iterates, into dX (x) and dY (y); the last step's
+  // A dX is in AdX[(iters - 1) % 2]
+  bnr_resolve_x<<<blocks_for((long long)nk), 256, 0, st>>>(
+      (long long)nk, K, b->accept, b->eta_prev, b->omega, b->c, b->X, b->AtY, b->L, b->U, b->dX);
+  bnr_resolve_y<<<blocks_for((long long)mk), 256, 0, st>>>(
+      (long long)mk, K, b->accept, b->eta_prev, b->omega, b->rl, b->ru, b->Y, b->AX,
+      ((iters - 1) & 1) ? b->AdX1 : b->AdX0, b->dY);
   // the bound: A^T Y, its terms, then per node (safebound.py:194-235)
   const int mblocks = (b->m + kRowsPerBlock - 1) / kRowsPerBlock;
   const int nblocks = (b->n + kRowsPerBlock - 1) / kRowsPerBlock;
-  launch_spmm(b->n, K, b->cp, b->ci, b->cx, b->Y, b->AtdY, st);
+  launch_spmm(b->n, K, b->cp, b->ci, b->cx, b->dY, b->AtdY, st);
   bnr_bound_terms<<<dim3(std::max(1, mblocks + nblocks), (K + 31) / 32), dim3(32, 8), 0, st>>>(
-      b->m, b->n, K, mblocks, mblocks + nblocks + 1, b->Y, b->rl, b->ru, b->c, b->AtdY, b->L, b->U,
-      b->part);
+      b->m, b->n, K, mblocks, mblocks + nblocks + 1, b->dY, b->rl, b->ru, b->c, b->AtdY, b->L,
+      b->U, b->part);
   bnr_bound_final<<<(K + 3) / 4, 128, 0, st>>>(K, mblocks, nblocks, b->part, b->obj_offset,
                                                b->obj_scale, b->bounds, b->empty);
-  count_launches(3);
+  count_launches(5);
   PDLP_CUDA(cudaGetLastError());
   // outputs; the step sizes stay with the engine for the next call
   if (bounds) PDLP_CUDA(cudaMemcpyAsync(bounds, b->bounds, sizeof(double) * K, outk, st));
-  if (x && nk) PDLP_CUDA(cudaMemcpyAsync(x, b->X, sizeof(double) * nk, outk, st));
-  if (y && mk) PDLP_CUDA(cudaMemcpyAsync(y, b->Y, sizeof(double) * mk, outk, st));
+  if (x && nk) PDLP_CUDA(cudaMemcpyAsync(x, b->dX, sizeof(double) * nk, outk, st));
+  if (y && mk) PDLP_CUDA(cudaMemcpyAsync(y, b->dY, sizeof(double) * mk, outk, st));
   if (infeasible) PDLP_CUDA(cudaMemcpyAsync(infeasible, b->empty, (size_t)K, outk, st));
   PDLP_CUDA(cudaMemcpyAsync(b->h_eta.data(), b->eta, sizeof(double) * K, cudaMemcpyDeviceToHost, st));
   PDLP_CUDA(cudaStreamSynchronize(st));

@@ -263,20 +263,6 @@ __device__ __forceinline__ double warp_blocks_sum(const double* __restrict__ par
   return lanes_total(s);
 }
 
-// Both slots at once, in the same order (one 16-byte load per block).
-__device__ __forceinline__ double2 warp_blocks_sum2(const double* __restrict__ part, int pstride,
-                                                    int node, int b0, int nb, int lane) {
-  const double2* p = reinterpret_cast<const double2*>(part + ((long long)node * pstride + b0) * 2);
-  double s0 = 0.0, s1 = 0.0;
-#pragma unroll 8
-  for (int b = lane; b < nb; b += 32) {
-    const double2 v = p[b];
-    s0 = add(s0, v.x);
-    s1 = add(s1, v.y);
-  }
-  return make_double2(lanes_total(s0), lanes_total(s1));
-}
-
 // Per node (one warp each): the step-size test's sums over the row blocks,
 // then the test and the next step size (bnr.py:244-270).  A taken trial sets
 // accept[node] (the next step's pend); eta_prev keeps the step it used.  fac holds the iteration's (1 - t^-growth,
@@ -293,9 +279,30 @@ __global__ void __launch_bounds__(128) bnr_accept(int k, int mblocks, int nblock
   const int node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (node >= k) return;            // whole warps leave together
   const int pstride = mblocks + nblocks + 1;
-  const double2 msums = warp_blocks_sum2(part, pstride, node, 0, mblocks, lane);
-  const double dyadx = msums.x, dydy = msums.y;
-  const double dxdx = warp_blocks_sum(part, pstride, node, mblocks, nblocks, 0, lane);
+  // the three sums, each in warp_blocks_sum's order, in one loop so that the
+  // loads of both sides are in flight together; their lane totals interleaved
+  // as three independent chains
+  const double* base = part + (long long)node * pstride * 2;
+  const double2* pm = reinterpret_cast<const double2*>(base);
+  const double* pn = base + 2 * (long long)mblocks;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  const int nmax = max(mblocks, nblocks);
+#pragma unroll 4
+  for (int b = lane; b < nmax; b += 32) {
+    if (b < mblocks) {
+      const double2 v = pm[b];
+      s0 = add(s0, v.x);
+      s1 = add(s1, v.y);
+    }
+    if (b < nblocks) s2 = add(s2, pn[2 * b]);
+  }
+  double dyadx = __shfl_sync(0xffffffffu, s0, 0), dydy = __shfl_sync(0xffffffffu, s1, 0),
+         dxdx = __shfl_sync(0xffffffffu, s2, 0);
+  for (int l = 1; l < 32; ++l) {
+    dyadx = add(dyadx, __shfl_sync(0xffffffffu, s0, l));
+    dydy = add(dydy, __shfl_sync(0xffffffffu, s1, l));
+    dxdx = add(dxdx, __shfl_sync(0xffffffffu, s2, l));
+  }
   if (lane != 0) return;
   const double om = omega[node];
   const double interaction = fabs(dyadx);

@@ -214,3 +214,59 @@ def test_ragged_node_tile_and_tiny_problem(require_gpu):
     same(r.x, ro.x)
     same(r.y, ro.y)
     assert np.isfinite(r.bounds).all()
+
+
+def test_device_pointers_give_the_host_results(require_gpu):
+    """The C entry point with device-resident bound sets and outputs
+    (PDLP_MEM_DEVICE) returns the same bits as with host arrays."""
+    import torch
+    from sovereign_moe_b200 import _lib
+    g = load("bnr_batch_s11")
+    K = int(g["K"])
+    e_host, e_dev = engine(g), engine(g)
+    r = e_host.solve_batch(g["L1"], g["U1"])
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")  # noqa: E731
+    dL, dU = dev(g["L1"]), dev(g["U1"])
+    db = torch.empty(K, dtype=torch.float64, device="cuda")
+    dx = torch.empty((int(g["n"]), K), dtype=torch.float64, device="cuda")
+    dy = torch.empty((int(g["m"]), K), dtype=torch.float64, device="cuda")
+    dinf = torch.empty(K, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    _lib.check(e_dev.lib.pdlp_bnr_solve_batch(
+        e_dev.h, K, dL.data_ptr(), dU.data_ptr(), None, None, int(g["iters"]), 0.3, 0.6,
+        db.data_ptr(), dx.data_ptr(), dy.data_ptr(), dinf.data_ptr(), _lib.PDLP_MEM_DEVICE))
+    same(db.cpu().numpy(), r.bounds)
+    same(dx.cpu().numpy(), r.x)
+    same(dy.cpu().numpy(), r.y)
+    assert np.array_equal(dinf.cpu().numpy().astype(bool), r.infeasible)
+
+
+def test_zero_iterations_bound_the_starting_point(require_gpu):
+    """iters = 0: the bound of each node's (clipped) warm start, as the
+    oracle computes it."""
+    g = load("bnr_small_s3")
+    e, o = engine(g, iters=0), oracle(g, iters=0)
+    warm = (np.asarray(g["x1"]), np.asarray(g["y1"]))
+    r, ro = e.solve_batch(g["L2"], g["U2"], warm=warm), o.solve_batch(g["L2"], g["U2"], warm=warm)
+    same(r.bounds, ro.bounds)
+    same(r.x, ro.x)
+    same(r.y, ro.y)
+
+
+def test_c_entry_point_refuses_bad_arguments(require_gpu):
+    from sovereign_moe_b200 import _lib
+    g = load("bnr_small_s3")
+    e = engine(g)
+    L = np.ascontiguousarray(g["L1"])
+    U = np.ascontiguousarray(g["U1"])
+    x = np.empty((int(g["n"]), 1))
+    call = lambda K, iters, wx=None, wy=None, mem=_lib.PDLP_MEM_HOST: e.lib.pdlp_bnr_solve_batch(  # noqa: E731
+        e.h, K, L.ctypes.data, U.ctypes.data, wx, wy, iters, 0.3, 0.6, None, None, None, None, mem)
+    assert call(0, 10) == _lib.PDLP_ERR_ARG
+    assert call(1, -1) == _lib.PDLP_ERR_ARG
+    assert call(1, 10, wx=x.ctypes.data) == _lib.PDLP_ERR_ARG
+    assert call(1, 10, mem=7) == _lib.PDLP_ERR_ARG
+    assert e.lib.pdlp_bnr_step_sizes(e.h, 1 << 20, None, None) == _lib.PDLP_ERR_ARG
+    # the engine still works after the refusals
+    r = e.solve_batch(g["L1"], g["U1"])
+    assert np.isfinite(r.bounds[~r.infeasible]).all()

@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_rows32_kernel(
     const long long rs = lane < nr ? (long long)__ldg(rp + r0 + lane) : 0LL;
     const long long re = lane < nr ? (long long)__ldg(rp + r0 + lane + 1) : 0LL;
     const bool is_long = lane < nr && re - rs > kLongRow;
-    if (is_long) long_rows[1 + atomicAdd(long_rows, 1)] = r0 + lane;
+    if (is_long) long_rows[2 + atomicAdd(long_rows, 1)] = r0 + lane;
     const unsigned long_mask = __ballot_sync(kAll, is_long);
     // mean length of the block's short rows -> lanes per row
     long long len = (lane < nr && !is_long) ? re - rs : 0;
@@ -97,12 +97,13 @@ __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_rows32_kernel(
 template <typename T>
 __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_long_rows_kernel(
     const int64_t* __restrict__ rp, const int* __restrict__ ri, const T* __restrict__ rx,
-    const T* __restrict__ x, T* __restrict__ y, const int* __restrict__ long_rows) {
+    const T* __restrict__ x, T* __restrict__ y, int* __restrict__ long_rows) {
   __shared__ T part[kSpmvWarps];
+  __shared__ bool last;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int count = long_rows[0];
   for (int k = blockIdx.x; k < count; k += gridDim.x) {
-    const int r = long_rows[1 + k];
+    const int r = long_rows[2 + k];
     const long long p0 = __ldg(rp + r), p1 = __ldg(rp + r + 1);
     T sum = T(0);
     for (long long base = p0 + 128LL * w; base < p1; base += 128LL * kSpmvWarps) {
@@ -131,12 +132,25 @@ __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_long_rows_kernel(
     }
     __syncthreads();
   }
+  // the last block to finish clears the count and this counter for the next
+  // call on the stream (every block read the count before it got here)
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(long_rows + 1, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    long_rows[0] = 0;
+    long_rows[1] = 0;
+  }
 }
 
-// The long-row list (a count, then row indices) of each (device, stream):
-// kept between calls and grown when a larger m comes, so a call allocates
-// nothing in the common case.  Calls on one stream are ordered by the
-// stream; calls on different streams use different lists.
+// The long-row list of each (device, stream): a count, a counter of finished
+// blocks, then row indices.  It is kept between calls and grown when a larger
+// m comes, so a call allocates nothing in the common case.  Both counters are
+// zeroed when the list is allocated, and the long-row kernel zeroes them again
+// at its end, so a call needs no reset of its own.  Calls on one stream are
+// ordered by the stream; calls on different streams use different lists.
 std::mutex spmv_mu;
 std::map<std::pair<int, cudaStream_t>, std::pair<int*, size_t>> spmv_lists;
 
@@ -153,6 +167,7 @@ int long_row_list(cudaStream_t st, size_t entries, int** out) {
     }
     const size_t n = std::max(entries, (size_t)1 << 16);
     PDLP_CUDA(cudaMalloc((void**)&slot.first, sizeof(int) * n));
+    PDLP_CUDA(cudaMemsetAsync(slot.first, 0, 2 * sizeof(int), st));
     slot.second = n;
   }
   *out = slot.first;
@@ -166,9 +181,8 @@ int launch_spmv(int m, const int64_t* rp, const int* ri, const T* rx, const T* x
   if (m == 0) return PDLP_OK;
   if (!rp || !ri || !rx || !x || !y) return fail(PDLP_ERR_ARG, "NULL pointer");
   int* long_rows = nullptr;
-  const int rc = long_row_list(st, (size_t)m + 1, &long_rows);
+  const int rc = long_row_list(st, (size_t)m + 2, &long_rows);
   if (rc != PDLP_OK) return rc;
-  PDLP_CUDA(cudaMemsetAsync(long_rows, 0, sizeof(int), st));
   const long long nblk = ((long long)m + 31) / 32;
   const int g = (int)std::min((nblk + kSpmvWarps - 1) / kSpmvWarps, 1LL << 30);
   spmv_rows32_kernel<T><<<g, kSpmvWarps * 32, 0, st>>>(m, rp, ri, rx, x, y, long_rows);

@@ -77,7 +77,12 @@ __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_rows32_kernel(
     const long long rs = lane < nr ? (long long)__ldg(rp + r0 + lane) : 0LL;
     const long long re = lane < nr ? (long long)__ldg(rp + r0 + lane + 1) : 0LL;
     const bool is_long = lane < nr && re - rs > kLongRow;
-    if (is_long) long_rows[2 + atomicAdd(long_rows, 1)] = r0 + lane;
+    if (is_long) {
+      // a count left over by a failed earlier call cannot push a write past
+      // the list (m + 2 entries): the slot is checked
+      const int slot = atomicAdd(long_rows, 1);
+      if (slot < m) long_rows[2 + slot] = r0 + lane;
+    }
     const unsigned long_mask = __ballot_sync(kAll, is_long);
     // mean length of the block's short rows -> lanes per row
     long long len = (lane < nr && !is_long) ? re - rs : 0;
@@ -97,13 +102,14 @@ __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_rows32_kernel(
 template <typename T>
 __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_long_rows_kernel(
     const int64_t* __restrict__ rp, const int* __restrict__ ri, const T* __restrict__ rx,
-    const T* __restrict__ x, T* __restrict__ y, int* __restrict__ long_rows) {
+    const T* __restrict__ x, T* __restrict__ y, int m, int* __restrict__ long_rows) {
   __shared__ T part[kSpmvWarps];
   __shared__ bool last;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int count = long_rows[0];
+  const int count = min(long_rows[0], m);
   for (int k = blockIdx.x; k < count; k += gridDim.x) {
     const int r = long_rows[2 + k];
+    if (r < 0 || r >= m) continue;    // only after a failed earlier call (block-uniform)
     const long long p0 = __ldg(rp + r), p1 = __ldg(rp + r + 1);
     T sum = T(0);
     for (long long base = p0 + 128LL * w; base < p1; base += 128LL * kSpmvWarps) {
@@ -186,7 +192,7 @@ int launch_spmv(int m, const int64_t* rp, const int* ri, const T* rx, const T* x
   const long long nblk = ((long long)m + 31) / 32;
   const int g = (int)std::min((nblk + kSpmvWarps - 1) / kSpmvWarps, 1LL << 30);
   spmv_rows32_kernel<T><<<g, kSpmvWarps * 32, 0, st>>>(m, rp, ri, rx, x, y, long_rows);
-  spmv_long_rows_kernel<T><<<592, kSpmvWarps * 32, 0, st>>>(rp, ri, rx, x, y, long_rows);
+  spmv_long_rows_kernel<T><<<592, kSpmvWarps * 32, 0, st>>>(rp, ri, rx, x, y, m, long_rows);
   count_launches(2);
   PDLP_CUDA(cudaGetLastError());
   return PDLP_OK;

@@ -15,21 +15,23 @@ namespace pdlp {
 
 // ---- grid barrier (bounded) ----------------------------------------------------
 //
-// Grid barrier on a monotonic arrival counter: the k-th barrier of a launch
-// is passed once the counter reaches k * nblocks (the host zeroes it before
-// each launch).  Arrival is an acquire-release add, the wait an acquire load,
-// so one atomic and one poll separate the last arrival from the release of
-// every block.  The wait is bounded in wall time: on timeout the block
-// records PDLP_ERR_BARRIER_TIMEOUT and every block leaves the kernel.
-__device__ bool grid_barrier(Control* ctl, unsigned target, long long timeout_ns, int* flag) {
+// Barrier of one block team on a monotonic arrival counter: the k-th barrier
+// of a launch is passed once the counter reaches k * (blocks of the team); the
+// host zeroes the counters before each launch.  Arrival is an acquire-release
+// add, the wait an acquire load, so one atomic and one poll separate the last
+// arrival from the release of every block.  The wait is bounded in wall time:
+// on timeout the block records PDLP_ERR_BARRIER_TIMEOUT and every block
+// leaves the kernel.
+__device__ bool grid_barrier(Control* ctl, unsigned* counter, unsigned target,
+                             long long timeout_ns, int* flag) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile int* err = &ctl->error;
     int ok = 1;
-    if (atom_add_acq_rel(&ctl->bar_count, 1u) + 1u < target) {
+    if (atom_add_acq_rel(counter, 1u) + 1u < target) {
       const long long t0 = global_ns();
       unsigned spins = 0;
-      while (ld_acquire(&ctl->bar_count) < target) {
+      while (ld_acquire(counter) < target) {
         if ((++spins & 255u) == 0u) {
           if (*err != 0) { ok = 0; break; }
           if (global_ns() - t0 > timeout_ns) {
@@ -47,7 +49,13 @@ __device__ bool grid_barrier(Control* ctl, unsigned target, long long timeout_ns
 }
 
 // One launch runs up to max_steps engine steps; every warp owns a fixed range
-// of row tiles and of column tiles for the whole launch.
+// of row tiles and of column tiles for the whole launch.  The blocks form
+// teams that do not wait for one another: each team's tiles are the tiles of
+// its own instances, and its barriers count only its blocks.  A team stops
+// when its instances are done, after max_steps, or when another team has
+// stopped (the host then re-plans the teams for what is left).  The team's
+// first block decides each next step between the step's two barriers, so
+// that every block of the team sees the same decision.
 extern __shared__ __align__(16) unsigned char g_smem[];
 constexpr size_t kSmemBytes = sizeof(WarpSmem) * kWarps + 16;
 
@@ -64,13 +72,16 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
   }
   __syncwarp();
   BulkPhase ph;
-  const unsigned nb = gridDim.x;
   const int gw = blockIdx.x * kWarps + warp;
   const int r0 = A.rwarp[gw], r1 = A.rwarp[gw + 1];
   const int c0 = A.cwarp[gw], c1 = A.cwarp[gw + 1];
   // the warp's first tile of each side stays in registers for the launch
   const Tile rfirst = r0 < r1 ? A.rtiles[r0] : Tile{};
   const Tile cfirst = c0 < c1 ? A.ctiles[c0] : Tile{};
+  const int team = A.block_team[blockIdx.x];
+  const bool leader = (int)blockIdx.x == A.team_first[team];
+  unsigned* const bar = &A.ctl->team_bar[team];
+  const unsigned nb = (unsigned)A.team_blocks[team];
   unsigned target = 0;
 #ifdef PDLP_TRACE
   // phase timestamps of the first and the last block for the first steps
@@ -82,9 +93,11 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
 #define PDLP_STAMP(step, k)
 #endif
   for (long long step = 0; step < A.max_steps; ++step) {
-    if (threadIdx.x == 0) flag = *(volatile int*)&A.ctl->active;
+    if (threadIdx.x == 0)
+      flag = *(volatile int*)&A.ctl->team_active[team] > 0 &&
+             *(volatile int*)&A.ctl->team_go[team] != 0;
     __syncthreads();
-    if (flag <= 0) return;
+    if (!flag) break;
     __syncthreads();
     PDLP_STAMP(step, 0);
     {
@@ -98,8 +111,12 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
     }
     PDLP_STAMP(step, 1);
     target += nb;
-    if (!grid_barrier(A.ctl, target, A.barrier_timeout_ns, &flag)) return;
+    if (!grid_barrier(A.ctl, bar, target, A.barrier_timeout_ns, &flag)) return;
     PDLP_STAMP(step, 2);
+    // the leader's decision for the next step, published by its arrival at
+    // the next barrier
+    if (leader && threadIdx.x == 0)
+      A.ctl->team_go[team] = *(volatile int*)&A.ctl->stop == 0;
     {
       Tile next = cfirst;
       PassCache pc;
@@ -111,9 +128,12 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
     }
     PDLP_STAMP(step, 3);
     target += nb;
-    if (!grid_barrier(A.ctl, target, A.barrier_timeout_ns, &flag)) return;
+    if (!grid_barrier(A.ctl, bar, target, A.barrier_timeout_ns, &flag)) return;
     PDLP_STAMP(step, 4);
   }
+  // this team is done for the launch: the other teams end theirs at their next
+  // step, so that the host can give this team's blocks to what is left
+  if (leader && threadIdx.x == 0) atomicExch(&A.ctl->stop, 1);
 #undef PDLP_STAMP
 }
 
@@ -422,6 +442,10 @@ struct pdlp_batch {
   Tile* d_ctiles = nullptr;
   int* d_rwarp = nullptr;
   int* d_cwarp = nullptr;
+  int* d_teams = nullptr;          // block_team[grid], team_blocks[T], team_first[T]
+  size_t cap_teams = 0;
+  int n_teams = 1;
+  std::vector<int> team_running;   // running instances per team, at the last rebuild
   int2* d_group_tiles = nullptr;
   double* d_partials = nullptr;
   double* d_gpartials = nullptr;
@@ -601,19 +625,99 @@ static int rebuild(pdlp_batch* b) {
   b->n_groups = (int)groups.size();
   b->n_rtiles = (int)rt.size();
   b->n_ctiles = (int)ct.size();
-  // persistent grid: enough warps for the larger tile list, at most what is co-resident
+  // persistent grid: enough warps for the larger tile list, at most what is
+  // co-resident.  With many instances, one team of blocks steps them all.
+  // With few (at most kTeamsFrom), each instance gets its own team, sized by
+  // its share of the work and its tile count, so that no instance waits at a
+  // barrier for another's tiles.
   const int max_blocks = std::max(1, b->sms * b->coop_blocks_per_sm);
-  const int want = (std::max(b->n_rtiles, b->n_ctiles) + kWarps - 1) / kWarps;
-  const int G = std::max(1, std::min(max_blocks, want));
-  b->grid = G;
-  std::vector<int> rwr, cwr;
-  block_ranges(rw, G * kWarps, rwr);
-  block_ranges(cw, G * kWarps, cwr);
+  std::vector<int> run;                       // running slots, in tile order
+  for (size_t s = 0; s < b->slots.size(); ++s)
+    if (b->slots[s].used && b->slots[s].running) run.push_back((int)s);
+  constexpr int kTeamsFrom = 48;
+  std::vector<int> tblocks;
+  if (b->cfg.persistent && run.size() >= 2 && (int)run.size() <= std::min(kTeamsFrom, kMaxTeams) &&
+      (int)run.size() <= max_blocks) {
+    double total = 0.0;
+    std::vector<double> w(run.size());
+    std::vector<int> want(run.size());
+    for (size_t k = 0; k < run.size(); ++k) {
+      const Slot& sl = b->slots[run[k]];
+      for (double v : sl.rtw) w[k] += v;
+      for (double v : sl.ctw) w[k] += v;
+      total += w[k];
+      const int tiles = std::max(sl.inst.rt_end - sl.inst.rt_begin, sl.inst.ct_end - sl.inst.ct_begin);
+      want[k] = std::max(1, (tiles + kWarps - 1) / kWarps);
+    }
+    tblocks.resize(run.size());
+    int used = 0;
+    for (size_t k = 0; k < run.size(); ++k) {
+      const int share = (int)((double)max_blocks * (total > 0 ? w[k] / total : 1.0 / run.size()));
+      tblocks[k] = std::max(1, std::min(want[k], share));
+      used += tblocks[k];
+    }
+    while (used > max_blocks) {               // rounding left too many: trim the largest
+      const size_t k = (size_t)(std::max_element(tblocks.begin(), tblocks.end()) - tblocks.begin());
+      if (tblocks[k] <= 1) break;
+      --tblocks[k];
+      --used;
+    }
+    if (used > max_blocks) tblocks.clear();   // cannot give every instance a block
+  }
+  std::vector<int> rwr, cwr, teams;
+  if (tblocks.empty()) {
+    const int want = (std::max(b->n_rtiles, b->n_ctiles) + kWarps - 1) / kWarps;
+    const int G = std::max(1, std::min(max_blocks, want));
+    b->grid = G;
+    block_ranges(rw, G * kWarps, rwr);
+    block_ranges(cw, G * kWarps, cwr);
+    b->n_teams = 1;
+    teams.assign(G, 0);
+    teams.push_back(G);                       // team_blocks
+    teams.push_back(0);                       // team_first
+    b->team_running.assign(1, (int)run.size());
+    for (int s : run) b->slots[s].inst.team = 0;
+  } else {
+    const int T = (int)run.size();
+    int G = 0;
+    for (int k = 0; k < T; ++k) G += tblocks[k];
+    b->grid = G;
+    b->n_teams = T;
+    rwr.clear();
+    cwr.clear();
+    teams.clear();
+    std::vector<int> first(T);
+    int fb = 0;
+    for (int k = 0; k < T; ++k) {
+      Slot& sl = b->slots[run[k]];
+      sl.inst.team = k;
+      first[k] = fb;
+      fb += tblocks[k];
+      for (int q = 0; q < tblocks[k]; ++q) teams.push_back(k);
+      // the team's warps split its own tiles, as one team splits all of them
+      const int r0 = sl.inst.rt_begin, r1 = sl.inst.rt_end;
+      const int c0 = sl.inst.ct_begin, c1 = sl.inst.ct_end;
+      std::vector<double> wr(rw.begin() + r0, rw.begin() + r1), wc(cw.begin() + c0, cw.begin() + c1);
+      std::vector<int> pr, pc;
+      block_ranges(wr, tblocks[k] * kWarps, pr);
+      block_ranges(wc, tblocks[k] * kWarps, pc);
+      for (int q = 0; q < tblocks[k] * kWarps; ++q) {
+        rwr.push_back(r0 + pr[q]);
+        cwr.push_back(c0 + pc[q]);
+      }
+    }
+    rwr.push_back(b->n_rtiles);
+    cwr.push_back(b->n_ctiles);
+    for (int k = 0; k < T; ++k) teams.push_back(tblocks[k]);
+    for (int k = 0; k < T; ++k) teams.push_back(first[k]);
+    b->team_running.assign(T, 1);
+  }
   int rc;
   if ((rc = ensure_capacity((void**)&b->d_rtiles, &b->cap_rtiles, rt.size(), sizeof(Tile)))) return rc;
   if ((rc = ensure_capacity((void**)&b->d_ctiles, &b->cap_ctiles, ct.size(), sizeof(Tile)))) return rc;
   if ((rc = ensure_capacity((void**)&b->d_rwarp, &b->cap_rwarp, rwr.size(), sizeof(int)))) return rc;
   if ((rc = ensure_capacity((void**)&b->d_cwarp, &b->cap_cwarp, cwr.size(), sizeof(int)))) return rc;
+  if ((rc = ensure_capacity((void**)&b->d_teams, &b->cap_teams, teams.size(), sizeof(int)))) return rc;
   if ((rc = ensure_capacity((void**)&b->d_partials, &b->cap_partials,
                             (rt.size() + ct.size()) * kNP, sizeof(double)))) return rc;
   if ((rc = ensure_capacity((void**)&b->d_group_tiles, &b->cap_groups, groups.size(), sizeof(int2)))) return rc;
@@ -626,6 +730,7 @@ static int rebuild(pdlp_batch* b) {
   if (!ct.empty()) PDLP_CUDA(cudaMemcpyAsync(b->d_ctiles, ct.data(), ct.size() * sizeof(Tile), cudaMemcpyHostToDevice, st));
   PDLP_CUDA(cudaMemcpyAsync(b->d_rwarp, rwr.data(), rwr.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   PDLP_CUDA(cudaMemcpyAsync(b->d_cwarp, cwr.data(), cwr.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  PDLP_CUDA(cudaMemcpyAsync(b->d_teams, teams.data(), teams.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   if (!groups.empty())
     PDLP_CUDA(cudaMemcpyAsync(b->d_group_tiles, groups.data(), groups.size() * sizeof(int2),
                               cudaMemcpyHostToDevice, st));
@@ -805,6 +910,7 @@ int pdlp_batch_destroy(pdlp_batch* b) {
   for (auto& a : b->spare) cudaFree(a.first);
   cudaFree(b->d_inst); cudaFree(b->d_state); cudaFree(b->d_counters); cudaFree(b->d_ctl);
   cudaFree(b->d_rtiles); cudaFree(b->d_ctiles); cudaFree(b->d_rwarp); cudaFree(b->d_cwarp);
+  cudaFree(b->d_teams);
   cudaFree(b->d_partials); cudaFree(b->d_group_tiles); cudaFree(b->d_gpartials);
   cudaFree(b->d_gcounters);
   cudaFree(b->d_raypart);
@@ -1071,13 +1177,21 @@ int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out) {
     A.rtiles = b->d_rtiles; A.n_rtiles = b->n_rtiles;
     A.ctiles = b->d_ctiles; A.n_ctiles = b->n_ctiles;
     A.rwarp = b->d_rwarp; A.cwarp = b->d_cwarp;
+    A.block_team = b->d_teams;
+    A.team_blocks = b->d_teams + b->grid;
+    A.team_first = b->d_teams + b->grid + b->n_teams;
     A.group_tiles = b->d_group_tiles; A.n_rgroups = b->n_rgroups; A.n_groups = b->n_groups;
     A.partials = b->d_partials; A.gpartials = b->d_gpartials; A.gcounters = b->d_gcounters;
     const int64_t chunk = std::min(left, kChunk);
     left -= chunk;
     A.max_steps = chunk;
     b->h_ctl->bar_count = 0; b->h_ctl->bar_gen = 0; b->h_ctl->active = b->n_running;
-    b->h_ctl->error = 0; b->h_ctl->error_where = 0;
+    b->h_ctl->error = 0; b->h_ctl->error_where = 0; b->h_ctl->stop = 0;
+    for (int t = 0; t < kMaxTeams; ++t) {
+      b->h_ctl->team_bar[t] = 0;
+      b->h_ctl->team_go[t] = 1;
+      b->h_ctl->team_active[t] = t < (int)b->team_running.size() ? b->team_running[t] : 0;
+    }
     PDLP_CUDA(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(Control), cudaMemcpyHostToDevice, st));
     PDLP_CUDA(cudaEventRecord(b->ev0, st));
     if (b->cfg.persistent) {

@@ -72,6 +72,7 @@ struct Inst {
   int ruiz_iters;           // 0 = no Ruiz
   int use_pc;
   int scale_none;
+  int team;                 // the block team that runs this instance (persistent launches)
   // matrix: CSR of A (row tiles) and CSR of A^T (column tiles), int32 pointers
   const int* rp; const int* ri;
   const int* cp; const int* ci;
@@ -148,14 +149,22 @@ struct Tile {
 
 constexpr int kGroupTiles = 64;          // tiles per reduction group
 
-// Engine-wide control block in device memory.
+constexpr int kMaxTeams = 64;            // block teams of one launch
+
+// Engine-wide control block in device memory.  The blocks of a launch form
+// teams (one team normally; one per instance when few instances are left):
+// each team steps at its own pace behind its own barrier.
 struct Control {
   unsigned int bar_count;
   unsigned int bar_gen;
   int active;               // instances still running
   int error;                // nonzero: a bounded wait gave up (code)
   int error_where;
-  unsigned int pad[3];
+  int stop;                 // set by a team that ends: every team leaves at its next step
+  unsigned int pad[2];
+  unsigned int team_bar[kMaxTeams];   // each team's barrier arrival counter
+  int team_active[kMaxTeams];         // each team's instances still running
+  int team_go[kMaxTeams];             // the team leader's decision for the next step
 };
 
 struct EngineArgs {
@@ -165,6 +174,9 @@ struct EngineArgs {
   const Tile* ctiles; int n_ctiles;
   const int* rwarp;         // persistent: warp w owns row tiles [rwarp[w], rwarp[w+1])
   const int* cwarp;
+  const int* block_team;    // persistent: team of each block
+  const int* team_blocks;   // [n_teams] blocks per team
+  const int* team_first;    // [n_teams] first block of each team (its leader)
   const int2* group_tiles;  // [n_groups]: tile range of each group (row groups first)
   int n_rgroups, n_groups;
   double* partials;         // [(n_rtiles + n_ctiles) * kNP] tile partials

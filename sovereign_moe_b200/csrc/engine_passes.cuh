@@ -989,6 +989,7 @@ __device__ void c_finish(const EngineArgs& A, const Inst& I, State* S, int cmode
       __threadfence();
       S->status = S->final_status;
       atomicSub(&A.ctl->active, 1);
+      atomicSub(&A.ctl->team_active[I.team], 1);
       break;
     }
     default: break;

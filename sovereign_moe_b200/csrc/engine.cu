@@ -627,14 +627,15 @@ static int rebuild(pdlp_batch* b) {
   b->n_ctiles = (int)ct.size();
   // persistent grid: enough warps for the larger tile list, at most what is
   // co-resident.  With many instances, one team of blocks steps them all.
-  // With few (at most kTeamsFrom), each instance gets its own team, sized by
-  // its share of the work and its tile count, so that no instance waits at a
-  // barrier for another's tiles.
+  // With fewer (at most kTeamsFrom), each instance gets its own team, sized
+  // by its share of the work and its tile count, so that no instance waits at
+  // a barrier for another's tiles.  On the 256-LP batch, teams from 48, 96,
+  // 160 and 256 running instances measured 679, 667, 662 and 682 ms.
   const int max_blocks = std::max(1, b->sms * b->coop_blocks_per_sm);
   std::vector<int> run;                       // running slots, in tile order
   for (size_t s = 0; s < b->slots.size(); ++s)
     if (b->slots[s].used && b->slots[s].running) run.push_back((int)s);
-  constexpr int kTeamsFrom = 48;
+  constexpr int kTeamsFrom = 160;
   std::vector<int> tblocks;
   if (b->cfg.persistent && run.size() >= 2 && (int)run.size() <= std::min(kTeamsFrom, kMaxTeams) &&
       (int)run.size() <= max_blocks) {

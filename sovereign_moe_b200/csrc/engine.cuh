@@ -149,7 +149,7 @@ struct Tile {
 
 constexpr int kGroupTiles = 64;          // tiles per reduction group
 
-constexpr int kMaxTeams = 64;            // block teams of one launch
+constexpr int kMaxTeams = 256;           // block teams of one launch
 
 // Engine-wide control block in device memory.  The blocks of a launch form
 // teams (one team normally; one per instance when few instances are left):

@@ -92,12 +92,13 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
 #else
 #define PDLP_STAMP(step, k)
 #endif
+  bool capped = true;                 // the loop ran its max_steps
   for (long long step = 0; step < A.max_steps; ++step) {
     if (threadIdx.x == 0)
       flag = *(volatile int*)&A.ctl->team_active[team] > 0 &&
              *(volatile int*)&A.ctl->team_go[team] != 0;
     __syncthreads();
-    if (!flag) break;
+    if (!flag) { capped = false; break; }
     __syncthreads();
     PDLP_STAMP(step, 0);
     {
@@ -131,9 +132,18 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
     if (!grid_barrier(A.ctl, bar, target, A.barrier_timeout_ns, &flag)) return;
     PDLP_STAMP(step, 4);
   }
-  // this team is done for the launch: the other teams end theirs at their next
-  // step, so that the host can give this team's blocks to what is left
-  if (leader && threadIdx.x == 0) atomicExch(&A.ctl->stop, 1);
+  // This team is done for the launch.  After its step cap the launch ends
+  // (the other teams leave at their next step).  A team whose instance is done
+  // ends the launch once an eighth of the blocks are idle, so that the host
+  // can give them to what is left without re-planning at every finish.
+  if (leader && threadIdx.x == 0) {
+    if (capped) {
+      atomicExch(&A.ctl->stop, 1);
+    } else if (*(volatile int*)&A.ctl->team_active[team] <= 0) {
+      const unsigned idle = atomicAdd(&A.ctl->idle, nb) + nb;
+      if (idle * 8u >= gridDim.x) atomicExch(&A.ctl->stop, 1);
+    }
+  }
 #undef PDLP_STAMP
 }
 
@@ -1187,7 +1197,7 @@ int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out) {
     left -= chunk;
     A.max_steps = chunk;
     b->h_ctl->bar_count = 0; b->h_ctl->bar_gen = 0; b->h_ctl->active = b->n_running;
-    b->h_ctl->error = 0; b->h_ctl->error_where = 0; b->h_ctl->stop = 0;
+    b->h_ctl->error = 0; b->h_ctl->error_where = 0; b->h_ctl->stop = 0; b->h_ctl->idle = 0;
     for (int t = 0; t < kMaxTeams; ++t) {
       b->h_ctl->team_bar[t] = 0;
       b->h_ctl->team_go[t] = 1;

@@ -160,8 +160,9 @@ struct Control {
   int active;               // instances still running
   int error;                // nonzero: a bounded wait gave up (code)
   int error_where;
-  int stop;                 // set by a team that ends: every team leaves at its next step
-  unsigned int pad[2];
+  int stop;                 // set to end the launch: every team leaves at its next step
+  unsigned int idle;        // blocks of teams whose instances are all done
+  unsigned int pad;
   unsigned int team_bar[kMaxTeams];   // each team's barrier arrival counter
   int team_active[kMaxTeams];         // each team's instances still running
   int team_go[kMaxTeams];             // the team leader's decision for the next step

@@ -597,6 +597,48 @@ static void make_groups(std::vector<Tile>& tiles, int t0, int t1, int group_base
   }
 }
 
+// The block teams of a persistent launch.  With many running instances one
+// team of blocks steps them all.  With fewer (at most kTeamsFrom), each
+// instance gets its own team, sized by its share of the work and its tile
+// count, so that no instance waits at a barrier for another's tiles.  On the
+// 256-LP batch, teams from 48, 96, 160 and 256 running instances measured
+// 679, 667, 662 and 682 ms.  Returns the blocks of each running instance's
+// team, in `run` order, or nothing for one team.
+static std::vector<int> plan_teams(const pdlp_batch* b, const std::vector<int>& run,
+                                   int max_blocks) {
+  constexpr int kTeamsFrom = 160;
+  std::vector<int> tblocks;
+  if (!b->cfg.persistent || run.size() < 2 ||
+      (int)run.size() > std::min(kTeamsFrom, kMaxTeams) || (int)run.size() > max_blocks)
+    return tblocks;
+  double total = 0.0;
+  std::vector<double> w(run.size());
+  std::vector<int> want(run.size());
+  for (size_t k = 0; k < run.size(); ++k) {
+    const Slot& sl = b->slots[run[k]];
+    for (double v : sl.rtw) w[k] += v;
+    for (double v : sl.ctw) w[k] += v;
+    total += w[k];
+    const int tiles = std::max(sl.inst.rt_end - sl.inst.rt_begin, sl.inst.ct_end - sl.inst.ct_begin);
+    want[k] = std::max(1, (tiles + kWarps - 1) / kWarps);    // one tile per warp
+  }
+  tblocks.resize(run.size());
+  int used = 0;
+  for (size_t k = 0; k < run.size(); ++k) {
+    const int share = (int)((double)max_blocks * (total > 0 ? w[k] / total : 1.0 / run.size()));
+    tblocks[k] = std::max(1, std::min(want[k], share));
+    used += tblocks[k];
+  }
+  while (used > max_blocks) {                 // rounding left too many: trim the largest
+    const size_t k = (size_t)(std::max_element(tblocks.begin(), tblocks.end()) - tblocks.begin());
+    if (tblocks[k] <= 1) break;
+    --tblocks[k];
+    --used;
+  }
+  if (used > max_blocks) tblocks.clear();     // cannot give every instance a block
+  return tblocks;
+}
+
 static int rebuild(pdlp_batch* b) {
   std::vector<Tile> rt, ct;
   std::vector<double> rw, cw;
@@ -636,45 +678,14 @@ static int rebuild(pdlp_batch* b) {
   b->n_rtiles = (int)rt.size();
   b->n_ctiles = (int)ct.size();
   // persistent grid: enough warps for the larger tile list, at most what is
-  // co-resident.  With many instances, one team of blocks steps them all.
-  // With fewer (at most kTeamsFrom), each instance gets its own team, sized
-  // by its share of the work and its tile count, so that no instance waits at
-  // a barrier for another's tiles.  On the 256-LP batch, teams from 48, 96,
-  // 160 and 256 running instances measured 679, 667, 662 and 682 ms.
+  // co-resident, in one team or in one team per instance (plan_teams)
   const int max_blocks = std::max(1, b->sms * b->coop_blocks_per_sm);
   std::vector<int> run;                       // running slots, in tile order
   for (size_t s = 0; s < b->slots.size(); ++s)
     if (b->slots[s].used && b->slots[s].running) run.push_back((int)s);
-  constexpr int kTeamsFrom = 160;
-  std::vector<int> tblocks;
-  if (b->cfg.persistent && run.size() >= 2 && (int)run.size() <= std::min(kTeamsFrom, kMaxTeams) &&
-      (int)run.size() <= max_blocks) {
-    double total = 0.0;
-    std::vector<double> w(run.size());
-    std::vector<int> want(run.size());
-    for (size_t k = 0; k < run.size(); ++k) {
-      const Slot& sl = b->slots[run[k]];
-      for (double v : sl.rtw) w[k] += v;
-      for (double v : sl.ctw) w[k] += v;
-      total += w[k];
-      const int tiles = std::max(sl.inst.rt_end - sl.inst.rt_begin, sl.inst.ct_end - sl.inst.ct_begin);
-      want[k] = std::max(1, (tiles + kWarps - 1) / kWarps);
-    }
-    tblocks.resize(run.size());
-    int used = 0;
-    for (size_t k = 0; k < run.size(); ++k) {
-      const int share = (int)((double)max_blocks * (total > 0 ? w[k] / total : 1.0 / run.size()));
-      tblocks[k] = std::max(1, std::min(want[k], share));
-      used += tblocks[k];
-    }
-    while (used > max_blocks) {               // rounding left too many: trim the largest
-      const size_t k = (size_t)(std::max_element(tblocks.begin(), tblocks.end()) - tblocks.begin());
-      if (tblocks[k] <= 1) break;
-      --tblocks[k];
-      --used;
-    }
-    if (used > max_blocks) tblocks.clear();   // cannot give every instance a block
-  }
+  const std::vector<int> tblocks = plan_teams(b, run, max_blocks);
+  // per warp tile ranges, then the team arrays: block_team[G], team_blocks[T],
+  // team_first[T]
   std::vector<int> rwr, cwr, teams;
   if (tblocks.empty()) {
     const int want = (std::max(b->n_rtiles, b->n_ctiles) + kWarps - 1) / kWarps;
@@ -684,8 +695,8 @@ static int rebuild(pdlp_batch* b) {
     block_ranges(cw, G * kWarps, cwr);
     b->n_teams = 1;
     teams.assign(G, 0);
-    teams.push_back(G);                       // team_blocks
-    teams.push_back(0);                       // team_first
+    teams.push_back(G);
+    teams.push_back(0);
     b->team_running.assign(1, (int)run.size());
     for (int s : run) b->slots[s].inst.team = 0;
   } else {
@@ -694,9 +705,6 @@ static int rebuild(pdlp_batch* b) {
     for (int k = 0; k < T; ++k) G += tblocks[k];
     b->grid = G;
     b->n_teams = T;
-    rwr.clear();
-    cwr.clear();
-    teams.clear();
     std::vector<int> first(T);
     int fb = 0;
     for (int k = 0; k < T; ++k) {

@@ -108,3 +108,34 @@ def test_planted_mistake_is_caught():
     o.damp = 0.5
     r1 = o.solve_batch(g["L1"], g["U1"])
     assert not np.array_equal(r1.bounds, g["bounds1"])
+
+
+def test_node_relaxation_workload_is_a_feasible_node_batch():
+    """The bench's node batch: a 20,000 x 30,000 LP with 8 entries per column,
+    equality rows met by an interior point of the [0, 10] box, and 128 bound
+    sets that each halve the box of 3 columns (a smaller copy here)."""
+    from sovereign_moe_b200.workloads import node_relaxation
+    prob, L, U = node_relaxation(m=400, n=600, per_col=8, nodes=16)
+    A = prob.A
+    assert (A.m, A.n) == (400, 600) and A.nnz == 600 * 8
+    assert np.array_equal(np.diff(A.cp), np.full(600, 8))
+    assert np.array_equal(prob.row_lb, prob.row_ub)
+    assert L.shape == U.shape == (600, 16)
+    assert ((L == 0) | (L == 5)).all() and ((U == 10) | (U == 5)).all() and (L <= U).all()
+    assert ((L != 0) | (U != 10)).sum(axis=0).tolist() == [3] * 16
+    # the oracle bounds every node with finite, deterministic values
+    o = BNROracle(A.rp, A.ri, A.rx, A.cp, A.ci, A.cx, prob.c, prob.row_lb, prob.row_ub,
+                  1.0, 0.0, batch=16, iters=20)
+    r = o.solve_batch(L, U)
+    assert np.isfinite(r.bounds).all() and not r.infeasible.any()
+    r2 = BNROracle(A.rp, A.ri, A.rx, A.cp, A.ci, A.cx, prob.c, prob.row_lb, prob.row_ub,
+                   1.0, 0.0, batch=16, iters=20).solve_batch(L, U)
+    assert np.array_equal(r.bounds, r2.bounds)
+
+
+def test_bnr_iteration_bytes():
+    """The algorithmic bytes the bnr bench line divides by its time."""
+    import bench
+    m, n, nnz, K = 20_000, 30_000, 240_000, 128
+    assert bench.bnr_bytes_per_iteration(m, n, nnz, K) == (
+        8 * (10 * n + 9 * m) * K + 2 * 12 * nnz + 8 * (m + 1) + 8 * (n + 1))

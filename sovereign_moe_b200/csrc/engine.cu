@@ -17,14 +17,27 @@ namespace pdlp {
 //
 // Barrier of one block team on a monotonic arrival counter: the k-th barrier
 // of a launch is passed once the counter reaches k * (blocks of the team); the
-// host zeroes the counters before each launch.  Arrival is an acquire-release
+// host zeroes the counters before each launch.  A team of one block needs only
+// its __syncthreads.  Arrival is an acquire-release
 // add, the wait an acquire load, so one atomic and one poll separate the last
 // arrival from the release of every block.  The wait is bounded in wall time:
 // on timeout the block records PDLP_ERR_BARRIER_TIMEOUT and every block
 // leaves the kernel.
 __device__ bool grid_barrier(Control* ctl, unsigned* counter, unsigned target,
-                             long long timeout_ns, int* flag) {
+                             long long timeout_ns, int* flag, bool alone) {
   __syncthreads();
+  if (alone) {
+    // A team of one block: no other block waits for it.  Thread 0's fence
+    // (after the __syncthreads that ordered every thread's writes before it)
+    // makes the block's writes visible at GPU scope, which the next pass's
+    // bulk copies read from, as the release of a multi-block barrier does.
+    if (threadIdx.x == 0) {
+      __threadfence();
+      *flag = *(volatile int*)&ctl->error == 0;
+    }
+    __syncthreads();
+    return *flag != 0;
+  }
   if (threadIdx.x == 0) {
     volatile int* err = &ctl->error;
     int ok = 1;
@@ -112,7 +125,7 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
     }
     PDLP_STAMP(step, 1);
     target += nb;
-    if (!grid_barrier(A.ctl, bar, target, A.barrier_timeout_ns, &flag)) return;
+    if (!grid_barrier(A.ctl, bar, target, A.barrier_timeout_ns, &flag, nb == 1u)) return;
     PDLP_STAMP(step, 2);
     // the leader's decision for the next step, published by its arrival at
     // the next barrier
@@ -129,7 +142,7 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
     }
     PDLP_STAMP(step, 3);
     target += nb;
-    if (!grid_barrier(A.ctl, bar, target, A.barrier_timeout_ns, &flag)) return;
+    if (!grid_barrier(A.ctl, bar, target, A.barrier_timeout_ns, &flag, nb == 1u)) return;
     PDLP_STAMP(step, 4);
   }
   // This team is done for the launch.  After its step cap the launch ends

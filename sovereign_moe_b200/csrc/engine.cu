@@ -17,12 +17,11 @@ namespace pdlp {
 //
 // Barrier of one block team on a monotonic arrival counter: the k-th barrier
 // of a launch is passed once the counter reaches k * (blocks of the team); the
-// host zeroes the counters before each launch.  A team of one block needs only
-// its __syncthreads.  Arrival is an acquire-release
+// host zeroes the counters before each launch.  Arrival is an acquire-release
 // add, the wait an acquire load, so one atomic and one poll separate the last
 // arrival from the release of every block.  The wait is bounded in wall time:
 // on timeout the block records PDLP_ERR_BARRIER_TIMEOUT and every block
-// leaves the kernel.
+// leaves the kernel.  A team of one block (`alone`) needs no counter.
 __device__ bool grid_barrier(Control* ctl, unsigned* counter, unsigned target,
                              long long timeout_ns, int* flag, bool alone) {
   __syncthreads();

@@ -75,3 +75,19 @@ def test_cpu_device_is_refused():
         solve_pdlp(single_small(0).problem, PDLPParams(device="cpu"))
     with pytest.raises(ValueError):
         solve_pdlp(single_small(0).problem, PDLPParams(device="tpu"))
+
+
+def test_bnr_engine_refuses_the_cpu_and_fails_loudly_without_a_gpu():
+    """The node-relaxation engine has no CPU path: device='cpu' is refused, and
+    without a GPU the library's create call fails with a clear error instead of
+    falling back."""
+    from types import SimpleNamespace
+    from sovereign_moe_b200.bnr import BNRConfig, BNREngine
+    from sovereign_moe_b200.workloads import node_relaxation
+    prob, _, _ = node_relaxation(m=40, n=60, per_col=4, nodes=2)
+    with pytest.raises(ValueError):
+        BNREngine(prob, SimpleNamespace(obj=1.0), BNRConfig(device="cpu"))
+    import torch
+    if not torch.cuda.is_available():
+        with pytest.raises(RuntimeError, match="GPU backend unavailable"):
+            BNREngine(prob, SimpleNamespace(obj=1.0), BNRConfig(batch=2, device="gpu"))

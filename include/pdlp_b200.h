@@ -180,7 +180,7 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* prob,
                      const pdlp_params* params, int32_t* slot_out);
 /* Advances every active slot by up to `max_steps` engine steps (a step is one
  * half-iteration pair: the A pass and the A^T pass).  *active_out receives the
- * number of slots still running.  With 160 or fewer slots running, each slot
+ * number of slots still running.  With 256 or fewer slots running, each slot
  * steps at its own pace on its own team of blocks, so one call may advance
  * some slots by fewer steps than others; call again until *active_out is 0. */
 int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out);

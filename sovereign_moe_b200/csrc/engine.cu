@@ -613,12 +613,13 @@ static void make_groups(std::vector<Tile>& tiles, int t0, int t1, int group_base
 // team of blocks steps them all.  With fewer (at most kTeamsFrom), each
 // instance gets its own team, sized by its share of the work and its tile
 // count, so that no instance waits at a barrier for another's tiles.  On the
-// 256-LP batch, teams from 48, 96, 160 and 256 running instances measured
-// 679, 667, 662 and 682 ms.  Returns the blocks of each running instance's
-// team, in `run` order, or nothing for one team.
+// 256-LP batch (engine time per batch, with the idle rule of the kernel),
+// teams from 160, 200 and 256 running instances measured 585, 571 and 541 ms.
+// Returns the blocks of each running instance's team, in `run` order, or
+// nothing for one team.
 static std::vector<int> plan_teams(const pdlp_batch* b, const std::vector<int>& run,
                                    int max_blocks) {
-  constexpr int kTeamsFrom = 160;
+  constexpr int kTeamsFrom = 256;
   std::vector<int> tblocks;
   if (!b->cfg.persistent || run.size() < 2 ||
       (int)run.size() > std::min(kTeamsFrom, kMaxTeams) || (int)run.size() > max_blocks)

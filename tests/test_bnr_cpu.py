@@ -139,3 +139,20 @@ def test_bnr_iteration_bytes():
     m, n, nnz, K = 20_000, 30_000, 240_000, 128
     assert bench.bnr_bytes_per_iteration(m, n, nnz, K) == (
         8 * (10 * n + 9 * m) * K + 2 * 12 * nnz + 8 * (m + 1) + 8 * (n + 1))
+
+
+def test_bench_workloads_are_seeded():
+    """The bench's synthetic inputs are the same on every machine: the same
+    seed gives the same arrays, another seed different ones."""
+    from sovereign_moe_b200.workloads import node_relaxation, uneven_batch
+    a = uneven_batch(seed=5, count=3, m_lo=50, m_hi=300)
+    b = uneven_batch(seed=5, count=3, m_lo=50, m_hi=300)
+    c = uneven_batch(seed=6, count=3, m_lo=50, m_hi=300)
+    for x, y in zip(a, b):
+        assert np.array_equal(x.problem.A.cx, y.problem.A.cx)
+        assert np.array_equal(x.problem.c, y.problem.c) and x.f_star == y.f_star
+    assert not all(np.array_equal(x.problem.c, z.problem.c) if x.problem.c.shape == z.problem.c.shape
+                   else False for x, z in zip(a, c))
+    p1, L1, U1 = node_relaxation(m=100, n=150, per_col=4, nodes=4)
+    p2, L2, U2 = node_relaxation(m=100, n=150, per_col=4, nodes=4)
+    assert np.array_equal(p1.A.cx, p2.A.cx) and np.array_equal(L1, L2) and np.array_equal(U1, U2)

@@ -268,22 +268,35 @@ class GpuArm:
                           torch.empty(k.problem.A.m, dtype=torch.float64).pin_memory(),
                           torch.empty(k.problem.A.n, dtype=torch.float64).pin_memory())
                          for k in lps]
+        # contiguous descriptor and parameter arrays for pdlp_batch_admit_many
+        n = len(lps)
+        self.dev_arrays = ((_lib.ProblemDesc * n)(*[d for _, d in self.dev]),
+                           (_lib.Params * n)(*self.params))
+        self.host_arrays = ((_lib.ProblemDesc * n)(*[d for _, d in self.host]),
+                            (_lib.Params * n)(*self.hparams))
+        self.single = BatchEngine(max_slots=1)
+        self.latencies = []
         self.engine_ms = 0.0
         self.engine_bytes = 0.0
         self.engine_launches = 0
         self.engine_kernels = 0
 
     def step(self, host=False):
+        """One batched step: admit every LP, run the batch to completion, fetch
+        and retire.  Also records each LP's time to tolerance from the start
+        of the step: the host's admission time plus the device time from the
+        first LP's first engine pass to this LP's end (device clock)."""
         ct, L, c = self.ctypes, self._lib, self.lib
         descs = self.host if host else self.dev
         prms = self.hparams if host else self.params
         outs = self.out_host if host else self.out_dev
         mem = L.PDLP_MEM_HOST if host else L.PDLP_MEM_DEVICE
-        slots = []
-        for (t, d), p in zip(descs, prms):
-            s = ct.c_int32(-1)
-            L.check(c.pdlp_batch_admit(self.eng.h, ct.byref(d), ct.byref(p), ct.byref(s)))
-            slots.append(s.value)
+        darr, parr = (self.host_arrays if host else self.dev_arrays)
+        t0 = time.perf_counter()
+        slot_arr = (ct.c_int32 * len(descs))()
+        L.check(c.pdlp_batch_admit_many(self.eng.h, len(descs), darr, parr, slot_arr, None))
+        slots = list(slot_arr)
+        admit_s = time.perf_counter() - t0
         active = ct.c_int32(1)
         while active.value > 0:
             k0 = c.pdlp_launch_count()
@@ -293,15 +306,64 @@ class GpuArm:
             self.engine_ms += ms
             self.engine_bytes += by
             self.engine_launches += 1
-        statuses = []
-        for s, (x, y, dd) in zip(slots, outs):
+        statuses, starts, ends, self.per_lp = [], [], [], []
+        for s, (x, y, dd), k in zip(slots, outs, self.lps):
             r = L.Result()
             L.check(c.pdlp_batch_poll(self.eng.h, s, ct.byref(r)))
             statuses.append(r.status)
+            starts.append(r.device_start_ns)
+            ends.append(r.device_end_ns)
+            self.per_lp.append({"m": int(k.problem.A.m), "n": int(k.problem.A.n),
+                                "nnz": int(k.problem.A.nnz), "iterations": int(r.iterations),
+                                "restarts": int(r.restarts), "start_ns": int(r.device_start_ns),
+                                "end_ns": int(r.device_end_ns)})
             L.check(c.pdlp_batch_fetch(self.eng.h, s, x.data_ptr(), y.data_ptr(), dd.data_ptr(),
                                        None, mem))
             L.check(c.pdlp_batch_retire(self.eng.h, s))
+        first = min(starts)
+        self.latencies = [admit_s + (e - first) * 1e-9 for e in ends]
         return statuses
+
+    def one_at_a_time(self, count=None):
+        """The plain discipline on the same mix: each LP alone on a one-slot
+        engine (admit from pinned host buffers, solve, fetch x/y/d to host,
+        retire), one after another.  Returns each LP's service time (s); with
+        every LP submitted at the start, LP i's time to tolerance is the sum
+        of the service times up to i (first come, first served)."""
+        ct, L, c = self.ctypes, self._lib, self.lib
+        h = self.single.h
+        service = []
+        todo = list(zip(self.host, self.hparams, self.out_host))[:count]
+        for (t, d), p, (x, y, dd) in todo:
+            t0 = time.perf_counter()
+            s = ct.c_int32(-1)
+            L.check(c.pdlp_batch_admit(h, ct.byref(d), ct.byref(p), ct.byref(s)))
+            active = ct.c_int32(1)
+            while active.value > 0:
+                L.check(c.pdlp_batch_step(h, 1 << 16, ct.byref(active)))
+            r = L.Result()
+            L.check(c.pdlp_batch_poll(h, s.value, ct.byref(r)))
+            if r.status != 0:
+                raise RuntimeError(f"one-at-a-time solve ended with status {r.status}")
+            L.check(c.pdlp_batch_fetch(h, s.value, x.data_ptr(), y.data_ptr(), dd.data_ptr(),
+                                       None, L.PDLP_MEM_HOST))
+            L.check(c.pdlp_batch_retire(h, s.value))
+            service.append(time.perf_counter() - t0)
+        return service
+
+    def public_one_at_a_time(self, count=None):
+        """The same mix through the public drop-in call, solve_pdlp(prob,
+        params), one LP after another (a fresh solve per call, as the
+        reference's server makes one per request).  Returns service times."""
+        from sovereign_moe_b200.pdlp import solve_pdlp
+        service = []
+        for k in self.lps[:count]:
+            t0 = time.perf_counter()
+            sol = solve_pdlp(k.problem, self.p)
+            if int(sol.status) != 0:
+                raise RuntimeError(f"solve_pdlp ended with status {sol.status}")
+            service.append(time.perf_counter() - t0)
+        return service
 
 
 def verify_batch(arm, lps):
@@ -393,6 +455,37 @@ def run_gpu(args, rank, world):
     e2e = N_LP * world / (e2e_ms / 1000.0)
     h2d = sum(h2d_bytes(k.problem) for k in lps)
     d2h = sum(8 * (2 * k.problem.A.n + k.problem.A.m) for k in lps)
+    lat_batched = list(arm.latencies)
+    if args.dump_lps and rank == 0:
+        with open(args.dump_lps, "w") as fh:
+            json.dump(arm.per_lp, fh)
+
+    # The plain discipline on the same mix, the denominator of the batched
+    # form's speed-up: one LP at a time on a one-slot engine, host buffers in
+    # and out like e2e (one warm pass over a few LPs first), then through the
+    # public solve_pdlp call.
+    from sovereign_moe_b200.serving import latency_summary
+    service_warm = arm.one_at_a_time(count=4)
+    barrier()
+    ev0.record()
+    service = arm.one_at_a_time()
+    ev1.record()
+    barrier()
+    one_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    one_rate = N_LP * world / (one_ms / 1000.0)
+    public = None
+    if not args.no_public:
+        arm.public_one_at_a_time(count=2)
+        barrier()
+        ev0.record()
+        pub_service = arm.public_one_at_a_time()
+        ev1.record()
+        barrier()
+        pub_ms = max_over_ranks(ev0.elapsed_time(ev1))
+        public = {"value": N_LP * world / (pub_ms / 1000.0), "unit": "solves/s",
+                  "ms": pub_ms, "service_s": latency_summary(pub_service),
+                  "call": "solve_pdlp(prob, PDLPParams(eps_abs=1e-6, eps_rel=1e-6)) per LP"}
+    del service_warm
 
     peak, peak_kind = load_peaks()
     achieved = eng_bytes / (eng_ms / 1000.0) / 1e9 if eng_ms > 0 else 0.0
@@ -409,7 +502,20 @@ def run_gpu(args, rank, world):
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": e2e / one_rate,
+            "vs_baseline_basis": ("e2e solves/s of the batched engine over the plain "
+                                  "one-LP-at-a-time GPU PDLP on the same 256 LPs (one-slot "
+                                  "engine, pinned host buffers in and out, same tolerance)"),
+            "latency_s": dict(latency_summary(lat_batched),
+                              definition=("time to rel KKT 1e-6 of each LP from the start of "
+                                          "the e2e step (admission of all 256 on the host, "
+                                          "then the LP's end on the device clock)")),
+            "one_at_a_time": {"value": one_rate, "unit": "solves/s", "ms_per_step": one_ms,
+                              "latency_s": dict(latency_summary(np.cumsum(service)),
+                                                definition=("every LP submitted at the start, "
+                                                            "served first come first served")),
+                              "service_s": latency_summary(service),
+                              "public_solve_pdlp": public},
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "lps_per_step": N_LP,
                        "rows": "log-uniform 50-5000", "cols": "U{2..8} x rows",
@@ -437,6 +543,7 @@ def run_gpu(args, rank, world):
         dist.barrier()
         dist.destroy_process_group()
     arm.eng.close()
+    arm.single.close()
     return 0
 
 
@@ -765,6 +872,10 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0,
                     help="seconds of CPU work per timed CPU sample")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--dump-lps", default=None,
+                    help="write each LP's size, iterations and device start/end (JSON)")
+    ap.add_argument("--no-public", action="store_true",
+                    help="skip the one-at-a-time pass through the public solve_pdlp")
     ap.add_argument("--workload", default="batch",
                     choices=["batch", "blend", "powerlaw", "serving", "engine-steps", "spmv",
                              "precision", "bnr"],

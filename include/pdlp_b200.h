@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PDLP_ABI_VERSION 2
+#define PDLP_ABI_VERSION 3
 
 /* ---- error codes ------------------------------------------------------- */
 #define PDLP_OK                   0
@@ -130,6 +130,11 @@ typedef struct pdlp_result {
     double scale_obj;              /* objective scale of the preconditioner    */
     int32_t history_len;           /* checks recorded in the history buffer    */
     double device_seconds;         /* engine time for this LP on the device    */
+    int64_t device_start_ns;       /* device clock (%globaltimer, ns) at the
+                                      LP's first engine pass, and at its end
+                                      (0 while running); comparable between
+                                      the LPs of one device                  */
+    int64_t device_end_ns;
 } pdlp_result;
 
 /* ---- library ---------------------------------------------------------- */
@@ -163,11 +168,24 @@ typedef struct pdlp_batch_config {
     int32_t persistent;         /* 1: one cooperative launch per call to
                                    pdlp_batch_step; 0: one launch per phase
                                    (replayed from a CUDA graph)             */
-    int32_t block_threads;      /* 0 = default (256)                        */
+    int32_t block_threads;      /* 0 = default (128); no other value is
+                                   accepted                                 */
     int32_t tile_rows;          /* 0 = default                              */
     int32_t tile_nnz;           /* 0 = default                              */
     int32_t lanes_override;     /* 0 = per-LP choice; else lanes per row    */
     int64_t memory_budget;      /* bytes the batch may hold; 0 = free HBM   */
+    int64_t barrier_timeout_us; /* wall-clock limit of every device-side wait
+                                   (team barriers, staging copies); 0 = 4 s.
+                                   A wait that runs out ends the step with
+                                   PDLP_ERR_BARRIER_TIMEOUT and the batch
+                                   refuses later calls (PDLP_ERR_STATE)     */
+    int32_t test_withhold_arrival; /* test hook, 0 = off.  1: the last block
+                                   of the first team of two or more blocks
+                                   leaves the kernel at its first barrier
+                                   without arriving, so the team's bounded
+                                   wait runs out (a flag nothing sets); it
+                                   exercises the timeout path without any
+                                   device fault                             */
 } pdlp_batch_config;
 
 void pdlp_batch_config_default(pdlp_batch_config* cfg);
@@ -178,11 +196,22 @@ int pdlp_batch_destroy(pdlp_batch* b);
  * batch unchanged. */
 int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* prob,
                      const pdlp_params* params, int32_t* slot_out);
-/* Advances every active slot by up to `max_steps` engine steps (a step is one
- * half-iteration pair: the A pass and the A^T pass).  *active_out receives the
- * number of slots still running.  With 256 or fewer slots running, each slot
- * steps at its own pace on its own team of blocks, so one call may advance
- * some slots by fewer steps than others; call again until *active_out is 0. */
+/* Admits `count` LPs (arrays of descriptors and parameters; params NULL for
+ * the defaults) with three host synchronisations in all instead of two per
+ * LP: one for the device pointer arrays (only when an LP is in device
+ * memory), one for the device checks' verdicts and one at the end.
+ * slots_out[i] and codes_out[i] (each optional) receive each LP's slot (-1
+ * when refused) and code; a refused LP leaves the others admitted.  Returns
+ * the first refusal's code (its message in pdlp_last_error) or PDLP_OK.
+ * No counterpart in the reference, which solves one LP per call. */
+int pdlp_batch_admit_many(pdlp_batch* b, int32_t count, const pdlp_problem_desc* probs,
+                          const pdlp_params* params, int32_t* slots_out, int32_t* codes_out);
+/* Advances every running slot by `max_steps` engine steps (a step is one
+ * half-iteration pair: the A pass and the A^T pass), or until it finishes.
+ * The call returns once every slot that was running has done its max_steps
+ * steps or finished; *active_out receives the number still running.  With
+ * 256 or fewer slots running, each slot steps at its own pace on its own team
+ * of blocks, in one or more launches. */
 int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out);
 /* Status and info of a slot (status PDLP_STATUS_RUNNING while running). */
 int pdlp_batch_poll(pdlp_batch* b, int32_t slot, pdlp_result* result);
@@ -201,6 +230,14 @@ int pdlp_batch_statuses(pdlp_batch* b, int32_t* status_out, int32_t n);
 int pdlp_batch_retire(pdlp_batch* b, int32_t slot);
 /* Requests the slot to stop at its next check (status INTERRUPTED). */
 int pdlp_batch_cancel(pdlp_batch* b, int32_t slot);
+/* The slot's preconditioner, the reference's Scaling (src/sovopt/numerics/
+ * scaling.py:60-108, built by scale_problem(method="pdlp"), scaling.py:374-478):
+ * row factors r (m), column factors c (n), both powers of two, with the scaled
+ * problem A' = diag(r) A diag(c), and the objective scale.  Pointers in
+ * `memory`; NULL skips.  Valid once the slot has left its preconditioning
+ * passes (it has iterated, or finished); PDLP_ERR_STATE before that. */
+int pdlp_batch_scaling(pdlp_batch* b, int32_t slot, double* row_scale, double* col_scale,
+                       double* obj_scale, int32_t memory);
 /* Device bytes a slot for this problem would take (admission planning). */
 int64_t pdlp_slot_bytes(int32_t m, int32_t n, int64_t nnz);
 /* Per-kernel timing of the last pdlp_batch_step: total device milliseconds

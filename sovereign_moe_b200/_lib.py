@@ -64,14 +64,16 @@ class Result(ctypes.Structure):
                 ("dual_obj", ctypes.c_double), ("step_size", ctypes.c_double),
                 ("primal_weight", ctypes.c_double), ("objective", ctypes.c_double),
                 ("scale_obj", ctypes.c_double), ("history_len", ctypes.c_int32),
-                ("device_seconds", ctypes.c_double)]
+                ("device_seconds", ctypes.c_double), ("device_start_ns", ctypes.c_int64),
+                ("device_end_ns", ctypes.c_int64)]
 
 
 class BatchConfig(ctypes.Structure):
     _fields_ = [("max_slots", ctypes.c_int32), ("persistent", ctypes.c_int32),
                 ("block_threads", ctypes.c_int32), ("tile_rows", ctypes.c_int32),
                 ("tile_nnz", ctypes.c_int32), ("lanes_override", ctypes.c_int32),
-                ("memory_budget", ctypes.c_int64)]
+                ("memory_budget", ctypes.c_int64), ("barrier_timeout_us", ctypes.c_int64),
+                ("test_withhold_arrival", ctypes.c_int32)]
 
 
 # Every symbol include/pdlp_b200.h declares, with its argument types.
@@ -88,12 +90,15 @@ SIGNATURES = {
     "pdlp_batch_destroy": ([_c_p], ctypes.c_int),
     "pdlp_batch_admit": ([_c_p, ctypes.POINTER(ProblemDesc), ctypes.POINTER(Params),
                           ctypes.POINTER(_i32)], ctypes.c_int),
+    "pdlp_batch_admit_many": ([_c_p, _i32, ctypes.POINTER(ProblemDesc), ctypes.POINTER(Params),
+                               _c_p, _c_p], ctypes.c_int),
     "pdlp_batch_step": ([_c_p, _i64, ctypes.POINTER(_i32)], ctypes.c_int),
     "pdlp_batch_poll": ([_c_p, _i32, ctypes.POINTER(Result)], ctypes.c_int),
     "pdlp_batch_fetch": ([_c_p, _i32, _c_p, _c_p, _c_p, _c_p, _i32], ctypes.c_int),
     "pdlp_batch_retire": ([_c_p, _i32], ctypes.c_int),
     "pdlp_batch_statuses": ([_c_p, _c_p, _i32], ctypes.c_int),
     "pdlp_batch_cancel": ([_c_p, _i32], ctypes.c_int),
+    "pdlp_batch_scaling": ([_c_p, _i32, _c_p, _c_p, ctypes.POINTER(_d), _i32], ctypes.c_int),
     "pdlp_slot_bytes": ([_i32, _i32, _i64], ctypes.c_int64),
     "pdlp_batch_last_timing": ([_c_p, ctypes.POINTER(_d), ctypes.POINTER(_d),
                                 ctypes.POINTER(_i64)], ctypes.c_int),

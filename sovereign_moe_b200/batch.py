@@ -30,7 +30,8 @@ class BatchEngine:
     """A slot table of device-resident LPs and the engine that advances them."""
 
     def __init__(self, max_slots=256, persistent=True, tile_rows=0, tile_nnz=0,
-                 lanes_override=0, memory_budget=0, stream=None):
+                 lanes_override=0, memory_budget=0, stream=None, barrier_timeout_us=0,
+                 test_withhold_arrival=False):
         self.lib = _lib.load()
         cfg = _lib.BatchConfig()
         self.lib.pdlp_batch_config_default(ctypes.byref(cfg))
@@ -42,6 +43,8 @@ class BatchEngine:
             cfg.tile_nnz = int(tile_nnz)
         cfg.lanes_override = int(lanes_override)
         cfg.memory_budget = int(memory_budget)
+        cfg.barrier_timeout_us = int(barrier_timeout_us)
+        cfg.test_withhold_arrival = 1 if test_withhold_arrival else 0
         h = ctypes.c_void_p()
         code = self.lib.pdlp_batch_create(ctypes.byref(cfg), stream, ctypes.byref(h))
         if code == _lib.PDLP_ERR_CUDA:
@@ -84,6 +87,35 @@ class BatchEngine:
         del keep, keep_v0
         self._meta[slot.value] = (prob, params, int(p.history_capacity), t0)
         return slot.value
+
+    def admit_many(self, probs, params: PDLPParams | None = None, power_start="reference"):
+        """Admit several LPs with three host synchronisations in all (instead
+        of two per LP).  Returns ``(slots, codes)``: the slot of each LP (-1
+        when refused) and its return code; a refused LP does not stop the
+        others."""
+        params = params or PDLPParams()
+        _check_device(params.device)
+        count = len(probs)
+        if count == 0:
+            return [], []
+        t0 = time.perf_counter()
+        descs = (_lib.ProblemDesc * count)()
+        prms = (_lib.Params * count)()
+        keep = []
+        for i, prob in enumerate(probs):
+            d, k = problem_desc(prob)
+            p, kv = params_struct(params, int(prob.A.n), power_start=power_start)
+            descs[i], prms[i] = d, p
+            keep.append((k, kv))
+        slots = np.full(count, -1, dtype=np.int32)
+        codes = np.zeros(count, dtype=np.int32)
+        self.lib.pdlp_batch_admit_many(self.h, count, descs, prms, slots.ctypes.data,
+                                       codes.ctypes.data)
+        del keep
+        for prob, s, p in zip(probs, slots, prms):
+            if s >= 0:
+                self._meta[int(s)] = (prob, params, int(p.history_capacity), t0)
+        return [int(s) for s in slots], [int(c) for c in codes]
 
     def step(self, max_steps=1 << 16):
         """Advance every running slot; returns how many are still running."""
@@ -129,6 +161,16 @@ class BatchEngine:
     def cancel(self, slot):
         _lib.check(self.lib.pdlp_batch_cancel(self.h, int(slot)))
 
+    def scaling(self, slot):
+        """The slot's preconditioner: (row factors, column factors, objective
+        scale), the reference's ``Scaling.row/col/obj``."""
+        prob = self._meta[slot][0]
+        r, c = np.empty(int(prob.A.m)), np.empty(int(prob.A.n))
+        s = ctypes.c_double()
+        _lib.check(self.lib.pdlp_batch_scaling(self.h, int(slot), r.ctypes.data, c.ctypes.data,
+                                               ctypes.byref(s), _lib.PDLP_MEM_HOST))
+        return r, c, s.value
+
     def last_timing(self):
         """(device ms, algorithmic PDHG bytes, PDHG iterations) of the last step."""
         ms, by, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
@@ -141,7 +183,9 @@ class BatchEngine:
 
     def solve_all(self, probs, params=None):
         """Admit every LP, run to completion, fetch and retire: list of Solutions."""
-        slots = [self.admit(p, params) for p in probs]
+        slots, codes = self.admit_many(probs, params)
+        for c in codes:
+            _lib.check(c)
         self.run()
         out = [self.fetch(s) for s in slots]
         for s in slots:

@@ -22,14 +22,21 @@ namespace pdlp {
 // arrival from the release of every block.  The wait is bounded in wall time:
 // on timeout the block records PDLP_ERR_BARRIER_TIMEOUT and every block
 // leaves the kernel.  A team of one block (`alone`) needs no counter.
+//
+// The next pass stages tiles and vectors with bulk asynchronous copies, which
+// read global memory through the async proxy, while the data was written with
+// ordinary stores (generic proxy), by this block or by others.  Neither the
+// barrier's acquire nor a __threadfence orders generic writes before async-
+// proxy reads, so the caller follows every barrier with a global proxy fence
+// in each thread that issues copies (fence_proxy_async_global).
 __device__ bool grid_barrier(Control* ctl, unsigned* counter, unsigned target,
-                             long long timeout_ns, int* flag, bool alone) {
+                             long long timeout_ns, int* flag, bool alone, bool withhold) {
   __syncthreads();
   if (alone) {
-    // A team of one block: no other block waits for it.  Thread 0's fence
-    // (after the __syncthreads that ordered every thread's writes before it)
-    // makes the block's writes visible at GPU scope, which the next pass's
-    // bulk copies read from, as the release of a multi-block barrier does.
+    // A team of one block: no other block waits for it.  The __syncthreads
+    // ordered every thread's writes before thread 0's fence, which makes them
+    // visible at GPU scope (to the finishers of later passes, which read with
+    // ld.global.cg) as the release of a multi-block barrier does.
     if (threadIdx.x == 0) {
       __threadfence();
       *flag = *(volatile int*)&ctl->error == 0;
@@ -37,6 +44,9 @@ __device__ bool grid_barrier(Control* ctl, unsigned* counter, unsigned target,
     __syncthreads();
     return *flag != 0;
   }
+  // test hook: this block leaves without arriving; the rest of the team waits
+  // until the bounded wait below runs out
+  if (withhold) return false;
   if (threadIdx.x == 0) {
     volatile int* err = &ctl->error;
     int ok = 1;
@@ -94,6 +104,8 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
   const bool leader = (int)blockIdx.x == A.team_first[team];
   unsigned* const bar = &A.ctl->team_bar[team];
   const unsigned nb = (unsigned)A.team_blocks[team];
+  const bool withhold = (int)blockIdx.x == A.withhold_block;
+  const long long budget = *(volatile int*)&A.ctl->team_budget[team];
   unsigned target = 0;
 #ifdef PDLP_TRACE
   // phase timestamps of the first and the last block for the first steps
@@ -104,13 +116,13 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
 #else
 #define PDLP_STAMP(step, k)
 #endif
-  bool capped = true;                 // the loop ran its max_steps
-  for (long long step = 0; step < A.max_steps; ++step) {
+  long long step = 0;
+  for (; step < budget; ++step) {
     if (threadIdx.x == 0)
       flag = *(volatile int*)&A.ctl->team_active[team] > 0 &&
              *(volatile int*)&A.ctl->team_go[team] != 0;
     __syncthreads();
-    if (!flag) { capped = false; break; }
+    if (!flag) break;
     __syncthreads();
     PDLP_STAMP(step, 0);
     {
@@ -124,7 +136,8 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
     }
     PDLP_STAMP(step, 1);
     target += nb;
-    if (!grid_barrier(A.ctl, bar, target, A.barrier_timeout_ns, &flag, nb == 1u)) return;
+    if (!grid_barrier(A.ctl, bar, target, A.barrier_timeout_ns, &flag, nb == 1u, withhold)) return;
+    if (lane == 0) fence_proxy_async_global();
     PDLP_STAMP(step, 2);
     // the leader's decision for the next step, published by its arrival at
     // the next barrier
@@ -141,17 +154,21 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
     }
     PDLP_STAMP(step, 3);
     target += nb;
-    if (!grid_barrier(A.ctl, bar, target, A.barrier_timeout_ns, &flag, nb == 1u)) return;
+    if (!grid_barrier(A.ctl, bar, target, A.barrier_timeout_ns, &flag, nb == 1u, withhold)) return;
+    if (lane == 0) fence_proxy_async_global();
     PDLP_STAMP(step, 4);
   }
-  // This team is done for the launch.  After its step cap the launch ends
-  // (the other teams leave at their next step).  A team whose instance is done
+  // This team is done for the launch; its leader reports the steps it ran.
+  // After the launch's step cap the launch ends (the other teams leave at
+  // their next step) and the host re-plans.  A team that spent the rest of
+  // the call's budget of steps just leaves.  A team whose instance is done
   // ends the launch once an eighth of the blocks are idle, so that the host
   // can give them to what is left without re-planning at every finish.
   if (leader && threadIdx.x == 0) {
-    if (capped) {
+    A.ctl->team_steps[team] = (int)step;
+    if (step == A.max_steps) {
       atomicExch(&A.ctl->stop, 1);
-    } else if (*(volatile int*)&A.ctl->team_active[team] <= 0) {
+    } else if (step < budget && *(volatile int*)&A.ctl->team_active[team] <= 0) {
       const unsigned idle = atomicAdd(&A.ctl->idle, nb) + nb;
       if (idle * 8u >= gridDim.x) atomicExch(&A.ctl->stop, 1);
     }
@@ -424,6 +441,7 @@ void plan_tiles(const int64_t* ptr, int nrows, int inst, int rows_cap, int nnz_c
 
 struct Slot {
   bool used = false;
+  bool reserved = false;      // taken by an admission in progress
   bool running = false;
   // infeasibility test (between launches): previous iterates, next check
   bool detect = false;
@@ -494,6 +512,13 @@ struct pdlp_batch {
   double last_ms = 0.0, last_bytes = 0.0;
   long long last_iters = 0;
   std::vector<long long> iters_before;
+  std::vector<long long> steps_left;   // per slot: steps it may still run in this call
+  size_t bytes_pending = 0;            // arenas of admissions in progress
+  int* h_errs = nullptr;               // pinned: admission verdicts, one per slot
+  State* h_init = nullptr;             // pinned: initial states, one per slot
+  int64_t* h_ptrs = nullptr;           // pinned: device pointer arrays read for admission
+  size_t cap_hptrs = 0;
+  int withhold_candidate = -1;         // last block of the first multi-block team
 };
 
 namespace pdlp {
@@ -707,6 +732,7 @@ static int rebuild(pdlp_batch* b) {
     block_ranges(rw, G * kWarps, rwr);
     block_ranges(cw, G * kWarps, cwr);
     b->n_teams = 1;
+    b->withhold_candidate = G >= 2 ? G - 1 : -1;
     teams.assign(G, 0);
     teams.push_back(G);
     teams.push_back(0);
@@ -718,6 +744,7 @@ static int rebuild(pdlp_batch* b) {
     for (int k = 0; k < T; ++k) G += tblocks[k];
     b->grid = G;
     b->n_teams = T;
+    b->withhold_candidate = -1;
     std::vector<int> first(T);
     int fb = 0;
     for (int k = 0; k < T; ++k) {
@@ -725,6 +752,7 @@ static int rebuild(pdlp_batch* b) {
       sl.inst.team = k;
       first[k] = fb;
       fb += tblocks[k];
+      if (b->withhold_candidate < 0 && tblocks[k] >= 2) b->withhold_candidate = fb - 1;
       for (int q = 0; q < tblocks[k]; ++q) teams.push_back(k);
       // the team's warps split its own tiles, as one team splits all of them
       const int r0 = sl.inst.rt_begin, r1 = sl.inst.rt_end;
@@ -824,146 +852,32 @@ static int infeasibility_test(pdlp_batch* b, Slot& sl, int* request) {
   return PDLP_OK;
 }
 
-extern "C" {
+// ---- admission ---------------------------------------------------------------
+//
+// An admission runs in three phases so that many LPs can share the host's
+// synchronisations: (1) admit_enqueue validates the arguments and the
+// pointer arrays on the host, takes an arena and a slot, and enqueues the
+// copies and the device check; (2) the caller reads every admission's
+// verdict back with one synchronisation; (3) admit_complete fills the slot
+// (descriptor, tiles, initial state) or gives the arena back.
 
-int pdlp_abi_version(void) { return PDLP_ABI_VERSION; }
+struct Pending {
+  int slot = -1;
+  void* arena = nullptr;
+  size_t arena_bytes = 0;
+  SlotLayout L{};
+  pdlp_params prm{};
+  const pdlp_problem_desc* P = nullptr;
+  const int64_t* rp = nullptr;     // host-readable pointer arrays
+  const int64_t* cp = nullptr;
+};
 
-int64_t pdlp_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
-
-const char* pdlp_last_error(void) { return g_err.c_str(); }
-
-void pdlp_params_default(pdlp_params* p) {
-  std::memset(p, 0, sizeof(*p));
-  p->eps_abs = 1e-8;
-  p->eps_rel = 1e-8;
-  p->feas_cap = 1e-6;
-  p->max_iter = 200000;
-  p->time_limit = 600.0;
-  p->check_every = 64;
-  p->stepsize_every = 8;
-  p->beta_sufficient = 0.2;
-  p->beta_necessary = 0.8;
-  p->beta_artificial = 0.36;
-  p->primal_weight_smoothing = 0.5;
-  p->scaling = PDLP_SCALING_PDLP;
-  p->power_start = nullptr;
-  p->time_used = 0.0;
-  p->history_capacity = 0;
-  p->detect_infeasibility = 0;
-  p->eps_infeasible = 1e-8;
-}
-
-void pdlp_batch_config_default(pdlp_batch_config* c) {
-  std::memset(c, 0, sizeof(*c));
-  c->max_slots = 1;
-  c->persistent = 1;
-  c->block_threads = kBlock;
-  c->tile_rows = default_tile_rows();
-  c->tile_nnz = default_tile_nnz();
-  c->lanes_override = 0;
-  c->memory_budget = 0;
-}
-
-int64_t pdlp_slot_bytes(int32_t m, int32_t n, int64_t nnz) {
-  return (int64_t)layout_for(m, n, nnz, true, true, 4096).total;
-}
-
-int pdlp_batch_create(const pdlp_batch_config* cfg, void* stream, pdlp_batch** out) {
-  if (!out) return fail(PDLP_ERR_ARG, "out is NULL");
-  *out = nullptr;
-  pdlp_batch_config c;
-  pdlp_batch_config_default(&c);
-  if (cfg) c = *cfg;
-  if (c.max_slots <= 0) return fail(PDLP_ERR_ARG, "max_slots must be positive");
-  if (c.block_threads == 0) c.block_threads = kBlock;
-  if (c.block_threads != kBlock) return fail(PDLP_ERR_ARG, "block_threads must be " + std::to_string(kBlock));
-  if (c.tile_rows <= 0) c.tile_rows = default_tile_rows();
-  if (c.tile_rows > kWTileRows) return fail(PDLP_ERR_ARG, "tile_rows exceeds " + std::to_string(kWTileRows));
-  if (c.tile_nnz <= 0) c.tile_nnz = default_tile_nnz();
-  if (c.tile_nnz > kWTileNnz) return fail(PDLP_ERR_ARG, "tile_nnz exceeds " + std::to_string(kWTileNnz));
-  if (c.lanes_override && (c.lanes_override & (c.lanes_override - 1)))
-    return fail(PDLP_ERR_ARG, "lanes_override must be a power of two");
-  pdlp_batch* b = new pdlp_batch();
-  b->stream = (cudaStream_t)stream;
-  b->cfg = c;
-  b->slots.resize(c.max_slots);
-  b->iters_before.assign(c.max_slots, 0);
-  int dev = 0;
-  cudaError_t e;
-  auto bail = [&](cudaError_t err, const char* what) {
-    pdlp_batch_destroy(b);
-    return cuda_fail(err, what);
-  };
-  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return bail(e, "cudaGetDevice");
-  if ((e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
-    return bail(e, "cudaDeviceGetAttribute");
-  int coop = 0;
-  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-  if ((e = cudaFuncSetAttribute(engine_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kSmemBytes)) != cudaSuccess)
-    return bail(e, "cudaFuncSetAttribute");
-  if ((e = cudaFuncSetAttribute(engine_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kSmemBytes)) != cudaSuccess)
-    return bail(e, "cudaFuncSetAttribute");
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->coop_blocks_per_sm, engine_persistent,
-                                                          kBlock, kSmemBytes)) != cudaSuccess)
-    return bail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-  if (!coop || b->coop_blocks_per_sm < 1) b->cfg.persistent = 0;
-  if ((e = cudaMalloc(&b->d_inst, sizeof(Inst) * c.max_slots)) != cudaSuccess) return bail(e, "cudaMalloc");
-  if ((e = cudaMalloc(&b->d_state, sizeof(State) * c.max_slots)) != cudaSuccess) return bail(e, "cudaMalloc");
-  if ((e = cudaMalloc(&b->d_counters, sizeof(unsigned) * 2 * c.max_slots)) != cudaSuccess) return bail(e, "cudaMalloc");
-  if ((e = cudaMalloc(&b->d_ctl, sizeof(Control))) != cudaSuccess) return bail(e, "cudaMalloc");
-  if ((e = cudaMallocHost(&b->h_ctl, sizeof(Control))) != cudaSuccess) return bail(e, "cudaMallocHost");
-  if ((e = cudaMalloc(&b->d_raypart, sizeof(double) * 16 * kRayBlocks)) != cudaSuccess)
-    return bail(e, "cudaMalloc");
-  if ((e = cudaMallocHost(&b->h_raypart, sizeof(double) * 16 * kRayBlocks)) != cudaSuccess)
-    return bail(e, "cudaMallocHost");
-  if ((e = cudaMallocHost(&b->h_state, sizeof(State) * c.max_slots)) != cudaSuccess) return bail(e, "cudaMallocHost");
-  cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2 * c.max_slots, b->stream);
-  cudaMemsetAsync(b->d_ctl, 0, sizeof(Control), b->stream);
-  cudaMemsetAsync(b->d_state, 0, sizeof(State) * c.max_slots, b->stream);
-  std::vector<Inst> zero(c.max_slots);
-  std::memset(zero.data(), 0, sizeof(Inst) * zero.size());
-  cudaMemcpyAsync(b->d_inst, zero.data(), sizeof(Inst) * zero.size(), cudaMemcpyHostToDevice, b->stream);
-  cudaEventCreate(&b->ev0);
-  cudaEventCreate(&b->ev1);
-  if (!b->cfg.persistent &&
-      (e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking)) != cudaSuccess)
-    return bail(e, "cudaStreamCreateWithFlags");
-  if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return bail(e, "cudaStreamSynchronize");
-  *out = b;
-  return PDLP_OK;
-}
-
-int pdlp_batch_destroy(pdlp_batch* b) {
-  if (!b) return PDLP_OK;
-  cudaStreamSynchronize(b->stream);
-  for (auto& s : b->slots) if (s.arena) cudaFree(s.arena);
-  for (auto& a : b->spare) cudaFree(a.first);
-  cudaFree(b->d_inst); cudaFree(b->d_state); cudaFree(b->d_counters); cudaFree(b->d_ctl);
-  cudaFree(b->d_rtiles); cudaFree(b->d_ctiles); cudaFree(b->d_rwarp); cudaFree(b->d_cwarp);
-  cudaFree(b->d_teams);
-  cudaFree(b->d_partials); cudaFree(b->d_group_tiles); cudaFree(b->d_gpartials);
-  cudaFree(b->d_gcounters);
-  cudaFree(b->d_raypart);
-  if (b->h_raypart) cudaFreeHost(b->h_raypart);
-  if (b->graph) cudaGraphExecDestroy(b->graph);
-  if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
-  if (b->h_ctl) cudaFreeHost(b->h_ctl);
-  if (b->h_state) cudaFreeHost(b->h_state);
-  if (b->ev0) cudaEventDestroy(b->ev0);
-  if (b->ev1) cudaEventDestroy(b->ev1);
-  delete b;
-  return PDLP_OK;
-}
-
-int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_params* params,
-                     int32_t* slot_out) {
+static int admit_args(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_params* params,
+                      pdlp_params* prm) {
   if (!b || !P) return fail(PDLP_ERR_ARG, "NULL batch or problem");
   if (b->broken) return fail(PDLP_ERR_STATE, "batch is unusable after a device wait timed out");
-  pdlp_params prm;
-  pdlp_params_default(&prm);
-  if (params) prm = *params;
+  pdlp_params_default(prm);
+  if (params) *prm = *params;
   const int m = P->m, n = P->n;
   const long long nnz = P->nnz;
   if (m < 0 || n < 0 || nnz < 0) return fail(PDLP_ERR_ARG, "negative dimension");
@@ -971,42 +885,43 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
   if (P->sense != 1 && P->sense != -1) return fail(PDLP_ERR_ARG, "sense must be 1 or -1");
   if (P->memory != PDLP_MEM_HOST && P->memory != PDLP_MEM_DEVICE)
     return fail(PDLP_ERR_ARG, "memory must be PDLP_MEM_HOST or PDLP_MEM_DEVICE");
-  if (prm.check_every <= 0 || prm.stepsize_every <= 0) return fail(PDLP_ERR_ARG, "check_every and stepsize_every must be positive");
-  if (prm.max_iter < 0) return fail(PDLP_ERR_ARG, "max_iter must be >= 0");
-  if (prm.scaling < 0 || prm.scaling > 3) return fail(PDLP_ERR_ARG, "unknown scaling method");
-  if (prm.precision != PDLP_PRECISION_FP64 && prm.precision != PDLP_PRECISION_FP32_SPMV)
+  if (prm->check_every <= 0 || prm->stepsize_every <= 0)
+    return fail(PDLP_ERR_ARG, "check_every and stepsize_every must be positive");
+  if (prm->max_iter < 0) return fail(PDLP_ERR_ARG, "max_iter must be >= 0");
+  if (prm->scaling < 0 || prm->scaling > 3) return fail(PDLP_ERR_ARG, "unknown scaling method");
+  if (prm->precision != PDLP_PRECISION_FP64 && prm->precision != PDLP_PRECISION_FP32_SPMV)
     return fail(PDLP_ERR_ARG, "unknown precision");
   if (!std::isfinite(P->obj_offset)) return fail(PDLP_ERR_NUMERICAL, "obj_offset is not finite");
-  int slot = -1;
-  for (size_t s = 0; s < b->slots.size(); ++s) if (!b->slots[s].used) { slot = (int)s; break; }
-  if (slot < 0) return fail(PDLP_ERR_STATE, "no free slot");
-  cudaStream_t st = b->stream;
+  if (!P->rp || !P->cp) return fail(PDLP_ERR_ARG, "rp/cp are NULL");
+  return PDLP_OK;
+}
 
-  // host copies of the pointer arrays: validation and tile planning
-  std::vector<int64_t> hrp, hcp;
-  const int64_t* rp = P->rp;
-  const int64_t* cp = P->cp;
-  if (!rp || !cp) return fail(PDLP_ERR_ARG, "rp/cp are NULL");
-  if (P->memory == PDLP_MEM_DEVICE) {
-    hrp.resize(m + 1); hcp.resize(n + 1);
-    PDLP_CUDA(cudaMemcpyAsync(hrp.data(), rp, sizeof(int64_t) * (m + 1), cudaMemcpyDeviceToHost, st));
-    PDLP_CUDA(cudaMemcpyAsync(hcp.data(), cp, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, st));
-    PDLP_CUDA(cudaStreamSynchronize(st));
-    rp = hrp.data(); cp = hcp.data();
-  }
+// Phase 1.  pd.P, pd.prm, pd.rp and pd.cp are set by the caller (the pointer
+// arrays already readable on the host).  On success the slot is reserved,
+// the arena taken and the copies and the check enqueued on the stream.
+static int admit_enqueue(pdlp_batch* b, Pending& pd) {
+  const pdlp_problem_desc* P = pd.P;
+  const int m = P->m, n = P->n;
+  const long long nnz = P->nnz;
   auto check_ptr = [&](const int64_t* p, int len) {
     if (p[0] != 0 || p[len] != nnz) return false;
     for (int i = 0; i < len; ++i) if (p[i + 1] < p[i]) return false;
     return true;
   };
-  if (!check_ptr(rp, m) || !check_ptr(cp, n))
+  if (!check_ptr(pd.rp, m) || !check_ptr(pd.cp, n))
     return fail(PDLP_ERR_ARG, "malformed compressed pointers (must start at 0, be non-decreasing and end at nnz)");
-
+  int slot = -1;
+  for (size_t s = 0; s < b->slots.size(); ++s)
+    if (!b->slots[s].used && !b->slots[s].reserved) { slot = (int)s; break; }
+  if (slot < 0) return fail(PDLP_ERR_STATE, "no free slot");
+  cudaStream_t st = b->stream;
+  const pdlp_params& prm = pd.prm;
   const int hist_cap = std::max(0, prm.history_capacity);
   const bool has_kind = P->kind != nullptr;
   const bool has_v0 = prm.power_start != nullptr;
   const bool f32 = prm.precision == PDLP_PRECISION_FP32_SPMV;
-  SlotLayout L = layout_for(m, n, nnz, has_kind, has_v0, hist_cap, f32);
+  pd.L = layout_for(m, n, nnz, has_kind, has_v0, hist_cap, f32);
+  const SlotLayout& L = pd.L;
   // a retired arena that holds the layout without wasting more than half of itself
   int best = -1;
   for (size_t i = 0; i < b->spare.size(); ++i) {
@@ -1017,7 +932,6 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
   }
   void* arena = nullptr;
   size_t arena_bytes = L.total;
-  cudaError_t e = cudaSuccess;
   if (best >= 0) {
     arena = b->spare[(size_t)best].first;
     arena_bytes = b->spare[(size_t)best].second;
@@ -1027,7 +941,8 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
     // a new arena: within the budget (spare arenas are released first if needed)
     auto fits = [&](bool* ok) -> int {
       if (b->cfg.memory_budget > 0) {
-        *ok = b->bytes_held + b->bytes_spare + L.total <= (size_t)b->cfg.memory_budget;
+        *ok = b->bytes_held + b->bytes_pending + b->bytes_spare + L.total <=
+              (size_t)b->cfg.memory_budget;
       } else {
         size_t fr = 0, tot = 0;
         PDLP_CUDA(cudaMemGetInfo(&fr, &tot));
@@ -1046,72 +961,92 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
       if ((frc = fits(&ok))) return frc;
     }
     if (!ok) return fail(PDLP_ERR_OOM, "admission refused: the LP does not fit the memory budget");
-    e = cudaMalloc(&arena, L.total);
+    const cudaError_t e = cudaMalloc(&arena, L.total);
     if (e != cudaSuccess) {
       cudaGetLastError();
       return fail(PDLP_ERR_OOM, std::string("admission refused: cudaMalloc: ") + cudaGetErrorString(e));
     }
   }
+  pd.slot = slot;
+  pd.arena = arena;
+  pd.arena_bytes = arena_bytes;
+  b->slots[slot].reserved = true;
+  b->bytes_pending += arena_bytes;
   char* base = (char*)arena;
   auto at = [&](size_t off) { return (void*)(base + off); };
   int rc = PDLP_OK;
-  auto give_back = [&]() {      // a refused LP's arena returns to the spares
-    b->spare.push_back({arena, arena_bytes});
-    b->bytes_spare += arena_bytes;
-  };
-  auto cleanup = [&](int code) { cudaStreamSynchronize(st); give_back(); return code; };
-
   const int mem = P->memory;
-  // pointers: copy int64 into scratch, convert to int32 with checks
-  State init{};
-  std::memset(&init, 0, sizeof(init));
   // the state's error word doubles as the validation flag
   int* err_flag = &b->d_state[slot].error;
   PDLP_CUDA(cudaMemsetAsync(&b->d_state[slot], 0, sizeof(State), st));
   long long* rp64 = (long long*)at(L.tmp64);
   long long* cp64 = rp64 + (m + 1);
-  if ((rc = copy_in(rp64, P->rp, sizeof(int64_t) * (m + 1), mem, st))) return cleanup(rc);
-  if ((rc = copy_in(cp64, P->cp, sizeof(int64_t) * (n + 1), mem, st))) return cleanup(rc);
-  if ((rc = copy_in(at(L.ri), P->ri, sizeof(int) * nnz, mem, st))) return cleanup(rc);
-  if ((rc = copy_in(at(L.ci), P->ci, sizeof(int) * nnz, mem, st))) return cleanup(rc);
-  if ((rc = copy_in(at(L.rx0), P->rx, sizeof(double) * nnz, mem, st))) return cleanup(rc);
-  if ((rc = copy_in(at(L.cx0), P->cx, sizeof(double) * nnz, mem, st))) return cleanup(rc);
-  if ((rc = copy_in(at(L.c0), P->c, sizeof(double) * n, mem, st))) return cleanup(rc);
-  if ((rc = copy_in(at(L.lo0), P->col_lb, sizeof(double) * n, mem, st))) return cleanup(rc);
-  if ((rc = copy_in(at(L.hi0), P->col_ub, sizeof(double) * n, mem, st))) return cleanup(rc);
-  if ((rc = copy_in(at(L.rl0), P->row_lb, sizeof(double) * m, mem, st))) return cleanup(rc);
-  if ((rc = copy_in(at(L.ru0), P->row_ub, sizeof(double) * m, mem, st))) return cleanup(rc);
-  if (has_kind && (rc = copy_in(at(L.kind), P->kind, (size_t)n, mem, st))) return cleanup(rc);
-  if (has_v0 && (rc = copy_in(at(L.v0), prm.power_start, sizeof(double) * n, mem, st))) return cleanup(rc);
-  {
-    AdmitTasks T;
-    T.rp64 = rp64; T.rp32 = (int*)at(L.rp32); T.m = m;
-    T.cp64 = cp64; T.cp32 = (int*)at(L.cp32); T.n = n;
-    T.ri = (const int*)at(L.ri); T.ci = (const int*)at(L.ci); T.nnz = nnz;
-    T.rx0 = (const double*)at(L.rx0); T.cx0 = (const double*)at(L.cx0);
-    T.c0 = (const double*)at(L.c0); T.lo0 = (const double*)at(L.lo0); T.hi0 = (const double*)at(L.hi0);
-    T.rl0 = (const double*)at(L.rl0); T.ru0 = (const double*)at(L.ru0);
-    T.err = err_flag;
-    const long long most = std::max<long long>({nnz, (long long)m + 1, (long long)n + 1});
-    const int gx = (int)std::max(1LL, std::min(1024LL, (most + 255) / 256));
-    admission_check<<<dim3(gx, 11), 256, 0, st>>>(T);
-    PDLP_CUDA(cudaGetLastError());
-    count_launches(1);
-  }
-  int herr = 0;
-  PDLP_CUDA(cudaMemcpyAsync(&herr, err_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
-  e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) { give_back(); return cuda_fail(e, "admission copies"); }
-  if (herr & 1) { give_back(); return fail(PDLP_ERR_ARG, "malformed sparse structure (pointer or index out of range)"); }
-  if (herr & 2) { give_back(); return fail(PDLP_ERR_NUMERICAL, "NaN in the data, or an infinite matrix entry or cost"); }
+  if ((rc = copy_in(rp64, P->rp, sizeof(int64_t) * (m + 1), mem, st))) return rc;
+  if ((rc = copy_in(cp64, P->cp, sizeof(int64_t) * (n + 1), mem, st))) return rc;
+  if ((rc = copy_in(at(L.ri), P->ri, sizeof(int) * nnz, mem, st))) return rc;
+  if ((rc = copy_in(at(L.ci), P->ci, sizeof(int) * nnz, mem, st))) return rc;
+  if ((rc = copy_in(at(L.rx0), P->rx, sizeof(double) * nnz, mem, st))) return rc;
+  if ((rc = copy_in(at(L.cx0), P->cx, sizeof(double) * nnz, mem, st))) return rc;
+  if ((rc = copy_in(at(L.c0), P->c, sizeof(double) * n, mem, st))) return rc;
+  if ((rc = copy_in(at(L.lo0), P->col_lb, sizeof(double) * n, mem, st))) return rc;
+  if ((rc = copy_in(at(L.hi0), P->col_ub, sizeof(double) * n, mem, st))) return rc;
+  if ((rc = copy_in(at(L.rl0), P->row_lb, sizeof(double) * m, mem, st))) return rc;
+  if ((rc = copy_in(at(L.ru0), P->row_ub, sizeof(double) * m, mem, st))) return rc;
+  if (has_kind && (rc = copy_in(at(L.kind), P->kind, (size_t)n, mem, st))) return rc;
+  if (has_v0 && (rc = copy_in(at(L.v0), prm.power_start, sizeof(double) * n, mem, st))) return rc;
+  AdmitTasks T;
+  T.rp64 = rp64; T.rp32 = (int*)at(L.rp32); T.m = m;
+  T.cp64 = cp64; T.cp32 = (int*)at(L.cp32); T.n = n;
+  T.ri = (const int*)at(L.ri); T.ci = (const int*)at(L.ci); T.nnz = nnz;
+  T.rx0 = (const double*)at(L.rx0); T.cx0 = (const double*)at(L.cx0);
+  T.c0 = (const double*)at(L.c0); T.lo0 = (const double*)at(L.lo0); T.hi0 = (const double*)at(L.hi0);
+  T.rl0 = (const double*)at(L.rl0); T.ru0 = (const double*)at(L.ru0);
+  T.err = err_flag;
+  const long long most = std::max<long long>({nnz, (long long)m + 1, (long long)n + 1});
+  const int gx = (int)std::max(1LL, std::min(1024LL, (most + 255) / 256));
+  admission_check<<<dim3(gx, 11), 256, 0, st>>>(T);
+  PDLP_CUDA(cudaGetLastError());
+  count_launches(1);
+  return PDLP_OK;
+}
 
+// Releases what a failed admission took (after its work on the stream is done).
+static void admit_abandon(pdlp_batch* b, Pending& pd) {
+  if (pd.slot >= 0) b->slots[pd.slot].reserved = false;
+  if (pd.arena) {
+    b->spare.push_back({pd.arena, pd.arena_bytes});
+    b->bytes_spare += pd.arena_bytes;
+    b->bytes_pending -= pd.arena_bytes;
+  }
+  pd.slot = -1;
+  pd.arena = nullptr;
+}
+
+// Phase 3: herr is the device check's verdict for this admission.  The
+// initial state is staged in b->h_init[slot] (pinned); the caller
+// synchronises the stream before that buffer is reused.
+static int admit_complete(pdlp_batch* b, Pending& pd, int herr) {
+  if (herr & 1) { admit_abandon(b, pd); return fail(PDLP_ERR_ARG, "malformed sparse structure (pointer or index out of range)"); }
+  if (herr & 2) { admit_abandon(b, pd); return fail(PDLP_ERR_NUMERICAL, "NaN in the data, or an infinite matrix entry or cost"); }
+  const pdlp_problem_desc* P = pd.P;
+  const pdlp_params& prm = pd.prm;
+  const SlotLayout& L = pd.L;
+  const int m = P->m, n = P->n;
+  const long long nnz = P->nnz;
+  const int slot = pd.slot;
+  const int hist_cap = std::max(0, prm.history_capacity);
+  const bool has_kind = P->kind != nullptr;
+  const bool has_v0 = prm.power_start != nullptr;
+  const bool f32 = prm.precision == PDLP_PRECISION_FP32_SPMV;
+  char* base = (char*)pd.arena;
+  auto at = [&](size_t off) { return (void*)(base + off); };
   Slot& S = b->slots[slot];
   S = Slot();
   S.used = true;
   S.running = true;
   S.m = m; S.n = n; S.nnz = nnz;
-  S.arena = arena;
-  S.bytes = arena_bytes;
+  S.arena = pd.arena;
+  S.bytes = pd.arena_bytes;
   Inst& I = S.inst;
   std::memset(&I, 0, sizeof(I));
   I.m = m; I.n = n; I.nnz = nnz;
@@ -1154,8 +1089,8 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
   I.check_every = prm.check_every; I.stepsize_every = prm.stepsize_every;
   I.beta_s = prm.beta_sufficient; I.beta_n = prm.beta_necessary; I.beta_a = prm.beta_artificial;
   I.theta = prm.primal_weight_smoothing;
-  plan_tiles(rp, m, slot, b->cfg.tile_rows, b->cfg.tile_nnz, S.rt, S.rtw);
-  plan_tiles(cp, n, slot, b->cfg.tile_rows, b->cfg.tile_nnz, S.ct, S.ctw);
+  plan_tiles(pd.rp, m, slot, b->cfg.tile_rows, b->cfg.tile_nnz, S.rt, S.rtw);
+  plan_tiles(pd.cp, n, slot, b->cfg.tile_rows, b->cfg.tile_nnz, S.ct, S.ctw);
   // algorithmic bytes of one PDHG iteration: value + index per
   // entry and pointer per row on both passes, one gathered word per column /
   // row, the vectors each pass reads and writes
@@ -1163,21 +1098,277 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_param
                                4.0 * (m + n) + 8.0 * (9.0 * m + 10.0 * n) + 4.0 * (m + n)
                          : 24.0 * (double)nnz + 4.0 * (m + 1) + 4.0 * (n + 1) +
                                8.0 * (10.0 * m + 11.0 * n);
-
+  State& init = b->h_init[slot];
+  std::memset(&init, 0, sizeof(init));
   init.status = PDLP_STATUS_RUNNING;
   init.final_status = PDLP_STATUS_RUNNING;
   if (I.ruiz_iters > 0) { init.rmode = R_RUIZ; init.cmode = C_RUIZ; }
   else { init.rmode = R_PC; init.cmode = C_PC; }
   init.eta = 1.0; init.omega = 1.0; init.s_obj = 1.0;
+  cudaStream_t st = b->stream;
   PDLP_CUDA(cudaMemcpyAsync(&b->d_state[slot], &init, sizeof(State), cudaMemcpyHostToDevice, st));
   PDLP_CUDA(cudaMemsetAsync(b->d_counters + 2 * slot, 0, 2 * sizeof(unsigned), st));
-  PDLP_CUDA(cudaStreamSynchronize(st));
-  b->bytes_held += arena_bytes;
+  b->bytes_pending -= pd.arena_bytes;
+  b->bytes_held += pd.arena_bytes;
   b->n_running += 1;
   b->iters_before[slot] = 0;
   b->dirty = true;
-  if (slot_out) *slot_out = slot;
+  S.reserved = false;
   return PDLP_OK;
+}
+
+// Admits count LPs with one synchronisation for the device pointer arrays
+// (when any are in device memory), one for the checks' verdicts and one at
+// the end.  codes[i] receives each LP's code and slots[i] its slot (-1 when
+// refused); the return value is the first failure's code (its message in
+// pdlp_last_error) or PDLP_OK.
+static int admit_many(pdlp_batch* b, int count, const pdlp_problem_desc* const* probs,
+                      const pdlp_params* const* params, int32_t* slots, int32_t* codes) {
+  if (!b) return fail(PDLP_ERR_ARG, "NULL batch");
+  if (count < 0 || (count > 0 && !probs)) return fail(PDLP_ERR_ARG, "bad count or NULL problem list");
+  if (count > (int)b->slots.size()) return fail(PDLP_ERR_STATE, "more LPs than slots");
+  std::vector<Pending> pd(count);
+  std::vector<int> code(count, PDLP_OK);
+  std::string first_msg;
+  int first = PDLP_OK;
+  auto note = [&](int i, int c) {
+    code[i] = c;
+    if (c != PDLP_OK && first == PDLP_OK) { first = c; first_msg = get_error(); }
+  };
+  cudaStream_t st = b->stream;
+  // device pointer arrays: one pinned staging area, one synchronisation
+  size_t need = 0;
+  for (int i = 0; i < count; ++i) {
+    pd[i].P = probs[i];
+    const int rc = admit_args(b, probs[i], params ? params[i] : nullptr, &pd[i].prm);
+    note(i, rc);
+    if (rc == PDLP_OK && probs[i]->memory == PDLP_MEM_DEVICE)
+      need += (size_t)probs[i]->m + 1 + (size_t)probs[i]->n + 1;
+  }
+  if (need > b->cap_hptrs) {
+    if (b->h_ptrs) cudaFreeHost(b->h_ptrs);
+    b->h_ptrs = nullptr;
+    b->cap_hptrs = 0;
+    PDLP_CUDA(cudaMallocHost(&b->h_ptrs, sizeof(int64_t) * need));
+    b->cap_hptrs = need;
+  }
+  size_t off = 0;
+  for (int i = 0; i < count; ++i) {
+    if (code[i] != PDLP_OK) continue;
+    const pdlp_problem_desc* P = probs[i];
+    if (P->memory == PDLP_MEM_DEVICE) {
+      int64_t* hr = b->h_ptrs + off;
+      int64_t* hc = hr + (P->m + 1);
+      off += (size_t)P->m + 1 + (size_t)P->n + 1;
+      PDLP_CUDA(cudaMemcpyAsync(hr, P->rp, sizeof(int64_t) * (P->m + 1), cudaMemcpyDeviceToHost, st));
+      PDLP_CUDA(cudaMemcpyAsync(hc, P->cp, sizeof(int64_t) * (P->n + 1), cudaMemcpyDeviceToHost, st));
+      pd[i].rp = hr;
+      pd[i].cp = hc;
+    } else {
+      pd[i].rp = P->rp;
+      pd[i].cp = P->cp;
+    }
+  }
+  if (need) PDLP_CUDA(cudaStreamSynchronize(st));
+  for (int i = 0; i < count; ++i) {
+    if (code[i] != PDLP_OK) continue;
+    const int rc = admit_enqueue(b, pd[i]);
+    if (rc != PDLP_OK) {
+      cudaStreamSynchronize(st);        // its enqueued copies end before the arena is reused
+      admit_abandon(b, pd[i]);
+      note(i, rc);
+    }
+  }
+  // every verdict in one read-back
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < count; ++i) {
+    b->h_errs[i] = 0;
+    if (code[i] == PDLP_OK && e == cudaSuccess)
+      e = cudaMemcpyAsync(&b->h_errs[i], &b->d_state[pd[i].slot].error, sizeof(int),
+                          cudaMemcpyDeviceToHost, st);
+  }
+  const cudaError_t e2 = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = e2;
+  if (e != cudaSuccess) {
+    for (int i = 0; i < count; ++i) if (code[i] == PDLP_OK) admit_abandon(b, pd[i]);
+    return cuda_fail(e, "admission copies");
+  }
+  for (int i = 0; i < count; ++i) {
+    if (code[i] != PDLP_OK) continue;
+    note(i, admit_complete(b, pd[i], b->h_errs[i]));
+  }
+  PDLP_CUDA(cudaStreamSynchronize(st));    // the initial states have left h_init
+  for (int i = 0; i < count; ++i) {
+    if (slots) slots[i] = code[i] == PDLP_OK ? pd[i].slot : -1;
+    if (codes) codes[i] = code[i];
+  }
+  if (first != PDLP_OK) set_error(first_msg);
+  return first;
+}
+
+extern "C" {
+
+int pdlp_abi_version(void) { return PDLP_ABI_VERSION; }
+
+int64_t pdlp_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+const char* pdlp_last_error(void) { return g_err.c_str(); }
+
+void pdlp_params_default(pdlp_params* p) {
+  std::memset(p, 0, sizeof(*p));
+  p->eps_abs = 1e-8;
+  p->eps_rel = 1e-8;
+  p->feas_cap = 1e-6;
+  p->max_iter = 200000;
+  p->time_limit = 600.0;
+  p->check_every = 64;
+  p->stepsize_every = 8;
+  p->beta_sufficient = 0.2;
+  p->beta_necessary = 0.8;
+  p->beta_artificial = 0.36;
+  p->primal_weight_smoothing = 0.5;
+  p->scaling = PDLP_SCALING_PDLP;
+  p->power_start = nullptr;
+  p->time_used = 0.0;
+  p->history_capacity = 0;
+  p->detect_infeasibility = 0;
+  p->eps_infeasible = 1e-8;
+}
+
+void pdlp_batch_config_default(pdlp_batch_config* c) {
+  std::memset(c, 0, sizeof(*c));
+  c->max_slots = 1;
+  c->persistent = 1;
+  c->block_threads = kBlock;
+  c->tile_rows = default_tile_rows();
+  c->tile_nnz = default_tile_nnz();
+  c->lanes_override = 0;
+  c->memory_budget = 0;
+  c->barrier_timeout_us = 0;
+  c->test_withhold_arrival = 0;
+}
+
+int64_t pdlp_slot_bytes(int32_t m, int32_t n, int64_t nnz) {
+  return (int64_t)layout_for(m, n, nnz, true, true, 4096).total;
+}
+
+int pdlp_batch_create(const pdlp_batch_config* cfg, void* stream, pdlp_batch** out) {
+  if (!out) return fail(PDLP_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  pdlp_batch_config c;
+  pdlp_batch_config_default(&c);
+  if (cfg) c = *cfg;
+  if (c.max_slots <= 0) return fail(PDLP_ERR_ARG, "max_slots must be positive");
+  if (c.block_threads == 0) c.block_threads = kBlock;
+  if (c.block_threads != kBlock) return fail(PDLP_ERR_ARG, "block_threads must be " + std::to_string(kBlock));
+  if (c.tile_rows <= 0) c.tile_rows = default_tile_rows();
+  if (c.tile_rows > kWTileRows) return fail(PDLP_ERR_ARG, "tile_rows exceeds " + std::to_string(kWTileRows));
+  if (c.tile_nnz <= 0) c.tile_nnz = default_tile_nnz();
+  if (c.tile_nnz > kWTileNnz) return fail(PDLP_ERR_ARG, "tile_nnz exceeds " + std::to_string(kWTileNnz));
+  if (c.lanes_override && (c.lanes_override & (c.lanes_override - 1)))
+    return fail(PDLP_ERR_ARG, "lanes_override must be a power of two");
+  if (c.barrier_timeout_us < 0) return fail(PDLP_ERR_ARG, "barrier_timeout_us must be >= 0");
+  pdlp_batch* b = new pdlp_batch();
+  b->stream = (cudaStream_t)stream;
+  b->cfg = c;
+  b->slots.resize(c.max_slots);
+  b->iters_before.assign(c.max_slots, 0);
+  b->steps_left.assign(c.max_slots, 0);
+  int dev = 0;
+  cudaError_t e;
+  auto bail = [&](cudaError_t err, const char* what) {
+    pdlp_batch_destroy(b);
+    return cuda_fail(err, what);
+  };
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return bail(e, "cudaGetDevice");
+  if ((e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+    return bail(e, "cudaDeviceGetAttribute");
+  int coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  if ((e = cudaFuncSetAttribute(engine_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kSmemBytes)) != cudaSuccess)
+    return bail(e, "cudaFuncSetAttribute");
+  if ((e = cudaFuncSetAttribute(engine_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kSmemBytes)) != cudaSuccess)
+    return bail(e, "cudaFuncSetAttribute");
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->coop_blocks_per_sm, engine_persistent,
+                                                          kBlock, kSmemBytes)) != cudaSuccess)
+    return bail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (!coop || b->coop_blocks_per_sm < 1) b->cfg.persistent = 0;
+  if ((e = cudaMalloc(&b->d_inst, sizeof(Inst) * c.max_slots)) != cudaSuccess) return bail(e, "cudaMalloc");
+  if ((e = cudaMalloc(&b->d_state, sizeof(State) * c.max_slots)) != cudaSuccess) return bail(e, "cudaMalloc");
+  if ((e = cudaMalloc(&b->d_counters, sizeof(unsigned) * 2 * c.max_slots)) != cudaSuccess) return bail(e, "cudaMalloc");
+  if ((e = cudaMalloc(&b->d_ctl, sizeof(Control))) != cudaSuccess) return bail(e, "cudaMalloc");
+  if ((e = cudaMallocHost(&b->h_ctl, sizeof(Control))) != cudaSuccess) return bail(e, "cudaMallocHost");
+  if ((e = cudaMalloc(&b->d_raypart, sizeof(double) * 16 * kRayBlocks)) != cudaSuccess)
+    return bail(e, "cudaMalloc");
+  if ((e = cudaMallocHost(&b->h_raypart, sizeof(double) * 16 * kRayBlocks)) != cudaSuccess)
+    return bail(e, "cudaMallocHost");
+  if ((e = cudaMallocHost(&b->h_state, sizeof(State) * c.max_slots)) != cudaSuccess) return bail(e, "cudaMallocHost");
+  if ((e = cudaMallocHost(&b->h_init, sizeof(State) * c.max_slots)) != cudaSuccess) return bail(e, "cudaMallocHost");
+  if ((e = cudaMallocHost(&b->h_errs, sizeof(int) * c.max_slots)) != cudaSuccess) return bail(e, "cudaMallocHost");
+  cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2 * c.max_slots, b->stream);
+  cudaMemsetAsync(b->d_ctl, 0, sizeof(Control), b->stream);
+  cudaMemsetAsync(b->d_state, 0, sizeof(State) * c.max_slots, b->stream);
+  std::vector<Inst> zero(c.max_slots);
+  std::memset(zero.data(), 0, sizeof(Inst) * zero.size());
+  cudaMemcpyAsync(b->d_inst, zero.data(), sizeof(Inst) * zero.size(), cudaMemcpyHostToDevice, b->stream);
+  cudaEventCreate(&b->ev0);
+  cudaEventCreate(&b->ev1);
+  if (!b->cfg.persistent &&
+      (e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return bail(e, "cudaStreamCreateWithFlags");
+  if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return bail(e, "cudaStreamSynchronize");
+  *out = b;
+  return PDLP_OK;
+}
+
+int pdlp_batch_destroy(pdlp_batch* b) {
+  if (!b) return PDLP_OK;
+  cudaStreamSynchronize(b->stream);
+  for (auto& s : b->slots) if (s.arena) cudaFree(s.arena);
+  for (auto& a : b->spare) cudaFree(a.first);
+  cudaFree(b->d_inst); cudaFree(b->d_state); cudaFree(b->d_counters); cudaFree(b->d_ctl);
+  cudaFree(b->d_rtiles); cudaFree(b->d_ctiles); cudaFree(b->d_rwarp); cudaFree(b->d_cwarp);
+  cudaFree(b->d_teams);
+  cudaFree(b->d_partials); cudaFree(b->d_group_tiles); cudaFree(b->d_gpartials);
+  cudaFree(b->d_gcounters);
+  cudaFree(b->d_raypart);
+  if (b->h_raypart) cudaFreeHost(b->h_raypart);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+  if (b->h_ctl) cudaFreeHost(b->h_ctl);
+  if (b->h_state) cudaFreeHost(b->h_state);
+  if (b->h_init) cudaFreeHost(b->h_init);
+  if (b->h_errs) cudaFreeHost(b->h_errs);
+  if (b->h_ptrs) cudaFreeHost(b->h_ptrs);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  delete b;
+  return PDLP_OK;
+}
+
+int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_params* params,
+                     int32_t* slot_out) {
+  if (!b || !P) return fail(PDLP_ERR_ARG, "NULL batch or problem");
+  int32_t slot = -1, code = PDLP_OK;
+  const int rc = admit_many(b, 1, &P, &params, &slot, &code);
+  if (rc == PDLP_OK && slot_out) *slot_out = slot;
+  return rc;
+}
+
+int pdlp_batch_admit_many(pdlp_batch* b, int32_t count, const pdlp_problem_desc* probs,
+                          const pdlp_params* params, int32_t* slots_out, int32_t* codes_out) {
+  if (!b) return fail(PDLP_ERR_ARG, "NULL batch");
+  if (count < 0 || (count > 0 && !probs)) return fail(PDLP_ERR_ARG, "bad count or NULL problem array");
+  if (count > (int32_t)b->slots.size()) return fail(PDLP_ERR_STATE, "more LPs than slots");
+  std::vector<const pdlp_problem_desc*> pp(count);
+  std::vector<const pdlp_params*> qq(count);
+  for (int i = 0; i < count; ++i) {
+    pp[i] = probs + i;
+    qq[i] = params ? params + i : nullptr;
+  }
+  return admit_many(b, count, pp.data(), qq.data(), slots_out, codes_out);
 }
 
 int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out) {
@@ -1197,14 +1388,23 @@ int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out) {
 #endif
   A.inst = b->d_inst; A.st = b->d_state;
   A.counters = b->d_counters; A.ctl = b->d_ctl;
-  A.barrier_timeout_ns = 4000000000LL;
+  A.barrier_timeout_ns = b->cfg.barrier_timeout_us > 0 ? b->cfg.barrier_timeout_us * 1000LL
+                                                       : 4000000000LL;
   A.n_inst = (int)b->slots.size();
-  // Chunks of at most kChunk steps: between chunks the host drops finished
-  // LPs from the tile lists and re-balances the blocks over what is left.
+  // Launches of at most kChunk steps: between launches the host drops
+  // finished LPs from the tile lists and re-balances the blocks over what is
+  // left.  Every running LP may advance max_steps steps in this call; each
+  // team's budget for a launch is what its LP has left (one team: all its LPs
+  // advance together and have the same budget left).
   const int64_t kChunk = 256;
-  int64_t left = max_steps;
+  for (size_t s = 0; s < b->slots.size(); ++s)
+    b->steps_left[s] = (b->slots[s].used && b->slots[s].running) ? std::max<int64_t>(max_steps, 0) : 0;
   double total_ms = 0.0;
-  while (left > 0 && b->n_running > 0) {
+  while (b->n_running > 0) {
+    int64_t most = 0;                 // the largest budget left among running LPs
+    for (size_t s = 0; s < b->slots.size(); ++s)
+      if (b->slots[s].used && b->slots[s].running) most = std::max<int64_t>(most, b->steps_left[s]);
+    if (most <= 0) break;
     if (b->dirty && (rc = rebuild(b))) return rc;
     A.rtiles = b->d_rtiles; A.n_rtiles = b->n_rtiles;
     A.ctiles = b->d_ctiles; A.n_ctiles = b->n_ctiles;
@@ -1214,15 +1414,23 @@ int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out) {
     A.team_first = b->d_teams + b->grid + b->n_teams;
     A.group_tiles = b->d_group_tiles; A.n_rgroups = b->n_rgroups; A.n_groups = b->n_groups;
     A.partials = b->d_partials; A.gpartials = b->d_gpartials; A.gcounters = b->d_gcounters;
-    const int64_t chunk = std::min(left, kChunk);
-    left -= chunk;
-    A.max_steps = chunk;
+    const int64_t chunk = std::min(most, kChunk);
+    A.max_steps = b->cfg.persistent ? kChunk : chunk;
+    A.withhold_block = (b->cfg.persistent && b->cfg.test_withhold_arrival) ? b->withhold_candidate : -1;
     b->h_ctl->bar_count = 0; b->h_ctl->bar_gen = 0; b->h_ctl->active = b->n_running;
     b->h_ctl->error = 0; b->h_ctl->error_where = 0; b->h_ctl->stop = 0; b->h_ctl->idle = 0;
     for (int t = 0; t < kMaxTeams; ++t) {
       b->h_ctl->team_bar[t] = 0;
       b->h_ctl->team_go[t] = 1;
       b->h_ctl->team_active[t] = t < (int)b->team_running.size() ? b->team_running[t] : 0;
+      b->h_ctl->team_budget[t] = 0;
+      b->h_ctl->team_steps[t] = 0;
+    }
+    for (size_t s = 0; s < b->slots.size(); ++s) {
+      const Slot& sl = b->slots[s];
+      if (!sl.used || !sl.running) continue;
+      const int t = b->n_teams > 1 ? sl.inst.team : 0;
+      b->h_ctl->team_budget[t] = (int)std::min<int64_t>(b->steps_left[s], kChunk);
     }
     PDLP_CUDA(cudaMemcpyAsync(b->d_ctl, b->h_ctl, sizeof(Control), cudaMemcpyHostToDevice, st));
     PDLP_CUDA(cudaEventRecord(b->ev0, st));
@@ -1309,6 +1517,8 @@ int pdlp_batch_step(pdlp_batch* b, int64_t max_steps, int32_t* active_out) {
     for (size_t s = 0; s < b->slots.size(); ++s) {
       Slot& sl = b->slots[s];
       if (!sl.used || !sl.running) continue;
+      b->steps_left[s] -= b->cfg.persistent ? b->h_ctl->team_steps[b->n_teams > 1 ? sl.inst.team : 0]
+                                            : chunk;
       const State& hs = b->h_state[s];
       long long d = hs.iters_done - b->iters_before[s];
       b->iters_before[s] = hs.iters_done;
@@ -1375,6 +1585,8 @@ int pdlp_batch_poll(pdlp_batch* b, int32_t slot, pdlp_result* r) {
   r->scale_obj = hs.s_obj;
   r->history_len = hs.hist_len;
   r->device_seconds = hs.t_end_ns > hs.t_start_ns ? (hs.t_end_ns - hs.t_start_ns) * 1e-9 : 0.0;
+  r->device_start_ns = hs.t_start_ns;
+  r->device_end_ns = hs.t_end_ns;
   return PDLP_OK;
 }
 
@@ -1422,6 +1634,34 @@ int pdlp_batch_retire(pdlp_batch* b, int32_t slot) {
   b->bytes_held -= s.bytes;
   s = Slot();
   b->dirty = true;
+  return PDLP_OK;
+}
+
+int pdlp_batch_scaling(pdlp_batch* b, int32_t slot, double* row_scale, double* col_scale,
+                       double* obj_scale, int32_t memory) {
+  if (!b) return fail(PDLP_ERR_ARG, "NULL batch");
+  if (slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
+    return fail(PDLP_ERR_ARG, "no such slot");
+  if (memory != PDLP_MEM_HOST && memory != PDLP_MEM_DEVICE)
+    return fail(PDLP_ERR_ARG, "memory must be PDLP_MEM_HOST or PDLP_MEM_DEVICE");
+  Slot& s = b->slots[slot];
+  cudaStream_t st = b->stream;
+  State hs;
+  PDLP_CUDA(cudaMemcpyAsync(&hs, &b->d_state[slot], sizeof(State), cudaMemcpyDeviceToHost, st));
+  PDLP_CUDA(cudaStreamSynchronize(st));
+  // the factors are final once the set-up pass that follows them has run
+  const bool scaling = hs.rmode == R_RUIZ || hs.rmode == R_PC || hs.rmode == R_APPLY ||
+                       hs.cmode == C_RUIZ || hs.cmode == C_PC || hs.cmode == C_APPLY;
+  if (hs.status == PDLP_STATUS_RUNNING && (scaling || hs.rmode == R_SETUP0))
+    return fail(PDLP_ERR_STATE, "the slot is still preconditioning");
+  const cudaMemcpyKind k = memory == PDLP_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  if (row_scale && s.m) PDLP_CUDA(cudaMemcpyAsync(row_scale, s.inst.rs, sizeof(double) * s.m, k, st));
+  if (col_scale && s.n) PDLP_CUDA(cudaMemcpyAsync(col_scale, s.inst.cs, sizeof(double) * s.n, k, st));
+  if (obj_scale) {
+    if (memory == PDLP_MEM_HOST) *obj_scale = hs.s_obj;
+    else PDLP_CUDA(cudaMemcpyAsync(obj_scale, &b->d_state[slot].s_obj, sizeof(double), k, st));
+  }
+  PDLP_CUDA(cudaStreamSynchronize(st));
   return PDLP_OK;
 }
 

@@ -166,6 +166,8 @@ struct Control {
   unsigned int team_bar[kMaxTeams];   // each team's barrier arrival counter
   int team_active[kMaxTeams];         // each team's instances still running
   int team_go[kMaxTeams];             // the team leader's decision for the next step
+  int team_budget[kMaxTeams];         // steps each team may run in this launch (host)
+  int team_steps[kMaxTeams];          // steps each team completed (its leader, at exit)
 };
 
 struct EngineArgs {
@@ -185,8 +187,10 @@ struct EngineArgs {
   unsigned int* gcounters;  // [n_groups] tiles done per group
   unsigned int* counters;   // [2 * n_inst] groups done per instance and side
   Control* ctl;
-  long long max_steps;
+  long long max_steps;       // the launch's step cap; reaching it ends the launch
   long long barrier_timeout_ns;
+  int withhold_block;       // test hook: this block leaves at its first barrier
+                            // without arriving (-1: none)
   int n_inst;
   long long* trace;         // tracing builds only: phase timestamps, else null
 };

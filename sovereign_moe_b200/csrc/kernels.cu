@@ -25,10 +25,19 @@ int grid_1d(long long n, int per = kT) {
 //
 // spmv_rows32_kernel: one warp per block of 32 consecutive rows.  Rows with
 // more than kLongRow entries are not summed here: the warp appends them to a
-// list (order immaterial) and leaves them to the second launch.  For the
-// others the warp picks L lanes per row from the block's own mean row length
-// (a power of two, 1..32), so short rows keep every lane busy without a
-// cross-lane scan.  Each lane sums its strided entries in order, a xor
+// list (order immaterial) and leaves them to the second launch.
+//
+// A block without long rows whose entries fit the warp's staging buffer
+// (kStageEntries; the common case for sparse LPs) is streamed: its entries
+// are one contiguous range of the CSR arrays, so the warp loads indices and
+// values with coalesced, mutually independent loads, gathers every x it needs
+// at once, and stages the products in shared memory.  Each lane then sums one
+// row from the buffer in storage order.  The latency of a block is two memory
+// round trips, however many rows it has.
+//
+// Other blocks (long rows, or more entries than the buffer) take the row-
+// group path: the warp picks L lanes per row from the block's mean row length
+// (a power of two, 1..32); each lane sums its strided entries in order, a xor
 // butterfly over the L lanes combines them, and 32/L rows run side by side.
 //
 // spmv_long_rows_kernel: one block of 8 warps per listed long row (grid-
@@ -38,6 +47,55 @@ int grid_1d(long long n, int per = kT) {
 // list order or the launch shape, and repeated calls give the same bits.
 constexpr int kSpmvWarps = 8;
 constexpr int kLongRow = 256;
+constexpr int kStageEntries = 512;     // entries a warp stages for one row block
+constexpr int kStageUnroll = 8;        // independent loads per lane in flight
+
+// The streamed block: entries [p0, p0 + cnt) of rows r0 .. r0 + nr - 1.
+template <typename T>
+__device__ __forceinline__ void spmv_block_staged(int r0, int nr, long long rs, long long re,
+                                                  long long p0, int cnt, int lane,
+                                                  const int* __restrict__ ri,
+                                                  const T* __restrict__ rx,
+                                                  const T* __restrict__ x, T* __restrict__ y,
+                                                  T* __restrict__ prod) {
+  for (int q0 = 0; q0 < cnt; q0 += kStageUnroll * 32) {
+    int idx[kStageUnroll];
+    T val[kStageUnroll];
+#pragma unroll
+    for (int u = 0; u < kStageUnroll; ++u) {
+      const int q = q0 + u * 32 + lane;
+      idx[u] = q < cnt ? __ldg(ri + p0 + q) : 0;
+      val[u] = q < cnt ? __ldg(rx + p0 + q) : T(0);
+    }
+    T xv[kStageUnroll];
+#pragma unroll
+    for (int u = 0; u < kStageUnroll; ++u) {
+      const int q = q0 + u * 32 + lane;
+      xv[u] = q < cnt ? __ldg(x + idx[u]) : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kStageUnroll; ++u) {
+      const int q = q0 + u * 32 + lane;
+      if (q < cnt) prod[q] = val[u] * xv[u];
+    }
+  }
+  __syncwarp();
+  if (lane < nr) {
+    const int e = (int)(re - p0);
+    int q = (int)(rs - p0);
+    T a = T(0);
+    for (; q + 3 < e; q += 4) {       // four loads in flight, the adds in storage order
+      const T v0 = prod[q], v1 = prod[q + 1], v2 = prod[q + 2], v3 = prod[q + 3];
+      a += v0;
+      a += v1;
+      a += v2;
+      a += v3;
+    }
+    for (; q < e; ++q) a += prod[q];
+    y[r0 + lane] = a;
+  }
+  __syncwarp();
+}
 
 template <typename T, int L>
 __device__ __forceinline__ void spmv_block_rows(int r0, int nr, long long rs, long long re,
@@ -68,6 +126,7 @@ __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_rows32_kernel(
     int m, const int64_t* __restrict__ rp, const int* __restrict__ ri,
     const T* __restrict__ rx, const T* __restrict__ x, T* __restrict__ y,
     int* __restrict__ long_rows) {
+  __shared__ T stage[kSpmvWarps][kStageEntries];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const long long nblk = ((long long)m + 31) / 32;
   const long long stride = (long long)gridDim.x * kSpmvWarps;
@@ -84,6 +143,12 @@ __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_rows32_kernel(
       if (slot < m) long_rows[2 + slot] = r0 + lane;
     }
     const unsigned long_mask = __ballot_sync(kAll, is_long);
+    const long long p0 = __shfl_sync(kAll, rs, 0);
+    const long long p1 = __shfl_sync(kAll, re, nr - 1);
+    if (long_mask == 0u && p1 - p0 <= kStageEntries) {
+      spmv_block_staged<T>(r0, nr, rs, re, p0, (int)(p1 - p0), lane, ri, rx, x, y, stage[w]);
+      continue;
+    }
     // mean length of the block's short rows -> lanes per row
     long long len = (lane < nr && !is_long) ? re - rs : 0;
 #pragma unroll

@@ -18,6 +18,7 @@ machine without a usable GPU raises ``RuntimeError("GPU backend unavailable
 from __future__ import annotations
 
 import ctypes
+import sys
 import time
 from dataclasses import dataclass, field
 
@@ -179,23 +180,49 @@ def solve_pdlp(prob, params: PDLPParams | None = None) -> Solution:
     return _to_solution(prob, params, res, x, y, d, hist, time.perf_counter() - t0)
 
 
+def _result_types(prob, params):
+    """The classes of the returned objects.
+
+    A caller that passes the reference's own ``Problem``
+    (``sovopt.core.problem``) gets the reference's ``Solution`` and ``Status``
+    back, and one that passes the reference's ``PDLPParams``
+    (``sovopt.lp.pdlp``) gets its ``PDLPInfo``, so code written against sovopt
+    keeps working unchanged (``isinstance`` checks, ``Status`` comparisons).
+    Any other caller gets this package's classes, which have the same fields
+    and integers.  Returns ``(Solution, Status, PDLPInfo)``; this engine's
+    extra ``device_seconds`` is set on the info as an attribute."""
+    sol_cls, st_cls, info_cls = Solution, Status, PDLPInfo
+    mod = sys.modules.get(type(prob).__module__)
+    if mod is not None and mod is not sys.modules[Solution.__module__]:
+        cand_s, cand_st = getattr(mod, "Solution", None), getattr(mod, "Status", None)
+        if isinstance(cand_s, type) and isinstance(cand_st, type):
+            sol_cls, st_cls = cand_s, cand_st
+    pmod = sys.modules.get(type(params).__module__)
+    if pmod is not None and pmod is not sys.modules[__name__]:
+        cand_i = getattr(pmod, "PDLPInfo", None)
+        if isinstance(cand_i, type):
+            info_cls = cand_i
+    return sol_cls, st_cls, info_cls
+
+
 def _to_solution(prob, params, res, x, y, d, hist, elapsed):
-    status = Status(int(res.status))
+    Sol, St, Info = _result_types(prob, params)
+    status = St(int(res.status))
     obj = float(np.asarray(prob.c, dtype=np.float64) @ x) + float(prob.obj_offset)
     h = hist[:5 * int(res.history_len)].reshape(-1, 5)
     history = [(int(r[0]), float(r[1]), float(r[2]), float(r[3]), float(r[4])) for r in h]
-    info = PDLPInfo(iterations=int(res.iterations), restarts=int(res.restarts),
-                    rejected_steps=int(res.rejected_steps), primal_res=res.primal_res,
-                    dual_res=res.dual_res, gap=res.gap, primal_obj=res.primal_obj,
-                    dual_obj=res.dual_obj, step_size=res.step_size,
-                    primal_weight=res.primal_weight, device="gpu", history=history,
-                    device_seconds=res.device_seconds)
+    info = Info(iterations=int(res.iterations), restarts=int(res.restarts),
+                rejected_steps=int(res.rejected_steps), primal_res=res.primal_res,
+                dual_res=res.dual_res, gap=res.gap, primal_obj=res.primal_obj,
+                dual_obj=res.dual_obj, step_size=res.step_size,
+                primal_weight=res.primal_weight, device="gpu", history=history)
+    info.device_seconds = res.device_seconds
     if params.verbose:
         for (k, pu, du, gu, pou) in history:
             if k % params.log_every == 0:
                 print(f"  it {k:>7d}  pres {pu:.2e}  dres {du:.2e}  gap {gu:.2e}  obj {pou:.10g}")
-    sol = Solution(status=status, x=x, objective=obj, y=y, reduced_costs=d,
-                   iterations=int(res.iterations), time=elapsed, method="pdlp[gpu]")
+    sol = Sol(status=status, x=x, objective=obj, y=y, reduced_costs=d,
+              iterations=int(res.iterations), time=elapsed, method="pdlp[gpu]")
     sol.log = history
     sol.dual_bound = obj
     sol.work_units = float(res.iterations)

@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_defaults_match_reference_params():
     lib = _lib.load()
-    assert lib.pdlp_abi_version() == 2
+    assert lib.pdlp_abi_version() == 3
     p = _lib.Params()
     lib.pdlp_params_default(ctypes.byref(p))
     ref = PDLPParams()
@@ -52,11 +52,23 @@ def test_abi_version_and_defaults_match_reference_params():
 def test_struct_layouts_match_the_header():
     # sizes of the C structs on x86-64 (natural alignment)
     assert ctypes.sizeof(_lib.ProblemDesc) == 4 + 4 + 8 + 12 * 8 + 8 + 4 + 4
-    assert ctypes.sizeof(_lib.BatchConfig) == 6 * 4 + 8
-    assert ctypes.sizeof(_lib.Result) == 8 + 3 * 8 + 9 * 8 + 8 + 8
+    # six int32, memory_budget, barrier_timeout_us, test_withhold_arrival (+pad)
+    assert ctypes.sizeof(_lib.BatchConfig) == 6 * 4 + 8 + 8 + 8
+    # ..., history_len (+pad), device_seconds, device_start_ns, device_end_ns
+    assert ctypes.sizeof(_lib.Result) == 8 + 3 * 8 + 9 * 8 + 8 + 8 + 2 * 8
     # eps..time_limit, check/stepsize, betas + smoothing, scaling (+pad), power_start,
     # time_used, history_capacity + precision, detect (+pad), eps_infeasible
     assert ctypes.sizeof(_lib.Params) == 5 * 8 + 8 + 4 * 8 + 8 + 8 + 8 + 8 + 8 + 8
+
+
+def test_batch_config_defaults():
+    lib = _lib.load()
+    c = _lib.BatchConfig()
+    lib.pdlp_batch_config_default(ctypes.byref(c))
+    assert c.block_threads == 128          # the only block size the engine accepts
+    assert c.persistent == 1 and c.max_slots == 1
+    assert c.barrier_timeout_us == 0       # 0 = the 4 s default
+    assert c.test_withhold_arrival == 0    # the timeout test hook is off
 
 
 def test_slot_bytes_grows_with_the_problem():

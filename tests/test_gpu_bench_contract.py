@@ -17,7 +17,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def test_headline_line_has_every_contract_key(require_gpu):
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--steps", "1",
-                          "--warmup", "3", "--no-cpu"], capture_output=True, text=True,
+                          "--warmup", "3", "--no-cpu", "--no-public"], capture_output=True,
+                         text=True,
                          cwd=ROOT, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
@@ -38,3 +39,8 @@ def test_headline_line_has_every_contract_key(require_gpu):
     assert r["traffic"] > 0 and r["kernel"] == "engine_persistent"
     assert d["gpu_launches"] > 0
     assert "sm_mhz" in d["clocks"]
+    # the plain one-LP-at-a-time arm on the same mix, and the latency percentiles
+    one = d["one_at_a_time"]
+    assert one["value"] > 0 and d["vs_baseline"] == pytest.approx(e["value"] / one["value"])
+    for lat in (d["latency_s"], one["latency_s"], one["service_s"]):
+        assert 0 < lat["p50"] <= lat["p99"]

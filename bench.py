@@ -646,8 +646,12 @@ def run_spmv(args):
     """The standalone CSR SpMV kernel (``pdlp_spmv_f64`` / ``_f32``, the
     reference Backend's ``spmv``) on the large single-LP matrices: the
     blending plan (200k x 600k, 3M nnz) and the power-law LP (1M x 3M, 10M
-    nnz at --scale 1), y = A x and y = A^T x.  L2 is flushed (a 256 MB write)
-    before every timed call; each call is timed alone with CUDA events."""
+    nnz at --scale 1), y = A x and y = A^T x.  Each call is timed alone with
+    CUDA events after an L2 flush: a 256 MB write followed by a 256 MB read,
+    so that the cache holds no dirty lines whose write-back would land in the
+    timed call.  Every variant of the row-block pass is timed, then the
+    autotuner's choice (``pdlp_spmv_tune_*``) on the same matrix."""
+    import ctypes
     import torch
     from sovereign_moe_b200 import _lib
     from sovereign_moe_b200.workloads import blending_plan, power_law
@@ -655,11 +659,17 @@ def run_spmv(args):
     peak, kind = load_peaks()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
+
+    def flush_l2():
+        flush.zero_()
+        flush.sum(dtype=torch.int64)
+
     mats = [("blending_plan_200k_x_600k", blending_plan(seed=0).problem)]
     sc = args.scale
     mats.append((f"power_law_{int(1e6 * sc)}x{int(3e6 * sc)}",
                  power_law(seed=0, m=int(1_000_000 * sc), n=int(3_000_000 * sc),
                            nnz=int(10_000_000 * sc)).problem))
+    names = {_lib.PDLP_SPMV_STREAMED: "streamed", _lib.PDLP_SPMV_ROW_GROUPS: "row_groups"}
     rows = []
     for name, prob in mats:
         A = prob.A
@@ -668,36 +678,50 @@ def run_spmv(args):
             for prec in ("fp64", "fp32"):
                 dt = torch.float64 if prec == "fp64" else torch.float32
                 es = 8 if prec == "fp64" else 4
-                fn = lib.pdlp_spmv_f64 if prec == "fp64" else lib.pdlp_spmv_f32
+                fn = lib.pdlp_spmv_ex_f64 if prec == "fp64" else lib.pdlp_spmv_ex_f32
+                tune = lib.pdlp_spmv_tune_f64 if prec == "fp64" else lib.pdlp_spmv_tune_f32
                 rp = torch.as_tensor(np.asarray(ptr, np.int64), device="cuda")
                 ri = torch.as_tensor(np.asarray(idx, np.int32), device="cuda")
                 rx = torch.as_tensor(np.asarray(val), device="cuda").to(dt)
                 x = torch.randn(c, dtype=torch.float64, device="cuda").to(dt)
                 y = torch.empty(r, dtype=dt, device="cuda")
-                call = lambda: _lib.check(fn(int(r), rp.data_ptr(), ri.data_ptr(),  # noqa: E731
-                                             rx.data_ptr(), x.data_ptr(), y.data_ptr(),
-                                             stream.cuda_stream))
-                for _ in range(3):
-                    call()
-                times = []
-                for _ in range(args.steps * 10):
-                    flush.zero_()
-                    e0, e1 = _sync_events(torch)
-                    e0.record()
-                    call()
-                    e1.record()
-                    e1.synchronize()
-                    times.append(e0.elapsed_time(e1))
                 nnz = int(idx.shape[0])
                 algo = (es + 4) * nnz + 8 * (r + 1) + es * c + es * r
-                ms = statistics.median(times)
+
+                def timed(variant):
+                    call = lambda: _lib.check(fn(variant, int(r), rp.data_ptr(), ri.data_ptr(),  # noqa: E731
+                                                 rx.data_ptr(), x.data_ptr(), y.data_ptr(),
+                                                 stream.cuda_stream))
+                    for _ in range(3):
+                        call()
+                    times = []
+                    for _ in range(args.steps * 10):
+                        flush_l2()
+                        e0, e1 = _sync_events(torch)
+                        e0.record()
+                        call()
+                        e1.record()
+                        e1.synchronize()
+                        times.append(e0.elapsed_time(e1))
+                    return statistics.median(times)
+
+                per = {names[v]: timed(v) for v in names}
+                best = ctypes.c_int32(0)
+                tms = (ctypes.c_double * 2)()
+                _lib.check(tune(int(r), rp.data_ptr(), ri.data_ptr(), rx.data_ptr(), x.data_ptr(),
+                                y.data_ptr(), stream.cuda_stream, 10, ctypes.byref(best), tms))
+                ms = per[names[best.value]]
                 rows.append({"matrix": name, "product": side, "dtype": prec, "rows": int(r),
-                             "nnz": nnz, "ms": ms, "algorithmic_bytes": algo,
-                             "GBps": algo / ms / 1e6, "frac_of_measured_hbm": algo / ms / 1e6 / peak})
+                             "nnz": nnz, "algorithmic_bytes": algo,
+                             "ms_per_variant": per, "tuned_variant": names[best.value],
+                             "tuner_ms_warm_l2": {"streamed": tms[0], "row_groups": tms[1]},
+                             "ms": ms, "GBps": algo / ms / 1e6,
+                             "frac_of_measured_hbm": algo / ms / 1e6 / peak})
                 del rp, ri, rx, x, y
     print(json.dumps({"metric": "SpMV HBM GB/s", "unit": "GB/s", "results": rows,
                       "peak_GBps": peak, "peak_source": kind,
-                      "l2": "flushed before every call (256 MB write)"}), flush=True)
+                      "l2": "flushed before every call (256 MB write, then 256 MB read)"}),
+          flush=True)
     return 0
 
 

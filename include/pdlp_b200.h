@@ -258,6 +258,32 @@ int pdlp_spmv_f64(int32_t m, const int64_t* rp, const int32_t* ri, const double*
                   const double* x, double* y, void* stream);
 int pdlp_spmv_f32(int32_t m, const int64_t* rp, const int32_t* ri, const float* rx,
                   const float* x, float* y, void* stream);
+/* The same with an explicit variant of the row-block pass (the plain calls
+ * use PDLP_SPMV_STREAMED).  STREAMED: a run of rows whose entries fit a warp's
+ * 256-entry buffer is loaded with independent coalesced loads, its products
+ * staged in shared memory and each row summed in storage order; other rows
+ * take the row-group path.  ROW_GROUPS: every row takes the row-group path
+ * (L lanes per row from the block's mean row length, strided sums then a
+ * xor butterfly).  Both give the same results up to the summation order. */
+#define PDLP_SPMV_AUTO        0
+#define PDLP_SPMV_STREAMED    1
+#define PDLP_SPMV_ROW_GROUPS  2
+int pdlp_spmv_ex_f64(int32_t variant, int32_t m, const int64_t* rp, const int32_t* ri,
+                     const double* rx, const double* x, double* y, void* stream);
+int pdlp_spmv_ex_f32(int32_t variant, int32_t m, const int64_t* rp, const int32_t* ri,
+                     const float* rx, const float* x, float* y, void* stream);
+/* The SpMV autotuner: times each variant on this matrix and these vectors
+ * (one warm call, then `reps` calls, 0 = 10, with CUDA events on `stream`),
+ * writes y = A x, and returns the fastest variant in *best_variant and each
+ * variant's milliseconds per call in ms_per_variant[2] (STREAMED, ROW_GROUPS;
+ * optional).  Synchronises the stream.  The reference has a fixed launch
+ * shape (backend.py:379-384); the caller keeps the choice per matrix. */
+int pdlp_spmv_tune_f64(int32_t m, const int64_t* rp, const int32_t* ri, const double* rx,
+                       const double* x, double* y, void* stream, int32_t reps,
+                       int32_t* best_variant, double* ms_per_variant);
+int pdlp_spmv_tune_f32(int32_t m, const int64_t* rp, const int32_t* ri, const float* rx,
+                       const float* x, float* y, void* stream, int32_t reps,
+                       int32_t* best_variant, double* ms_per_variant);
 /* Y = A X, X dense (ncols, k) row-major, batch index fastest (backend.py:386-400) */
 int pdlp_spmm_f64(int32_t m, int32_t k, const int64_t* rp, const int32_t* ri,
                   const double* rx, const double* X, double* Y, void* stream);

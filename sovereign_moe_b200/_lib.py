@@ -25,6 +25,10 @@ PDLP_ERR_BOUNDS = -7
 PDLP_MEM_DEVICE = 0
 PDLP_MEM_HOST = 1
 
+PDLP_SPMV_AUTO = 0
+PDLP_SPMV_STREAMED = 1
+PDLP_SPMV_ROW_GROUPS = 2
+
 PDLP_STATUS_RUNNING = -1
 PDLP_SLOT_FREE = -2
 
@@ -104,6 +108,12 @@ SIGNATURES = {
                                 ctypes.POINTER(_i64)], ctypes.c_int),
     "pdlp_spmv_f64": ([_i32, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
     "pdlp_spmv_f32": ([_i32, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
+    "pdlp_spmv_ex_f64": ([_i32, _i32, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
+    "pdlp_spmv_ex_f32": ([_i32, _i32, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
+    "pdlp_spmv_tune_f64": ([_i32, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _i32, ctypes.POINTER(_i32),
+                            _c_p], ctypes.c_int),
+    "pdlp_spmv_tune_f32": ([_i32, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _i32, ctypes.POINTER(_i32),
+                            _c_p], ctypes.c_int),
     "pdlp_spmm_f64": ([_i32, _i32, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
     "pdlp_primal_step": ([_i32, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _d, _c_p], ctypes.c_int),
     "pdlp_dual_step": ([_i32, _c_p, _c_p, _c_p, _c_p, _c_p, _d, _c_p], ctypes.c_int),

@@ -28,7 +28,7 @@ def _torch():
 class Backend:
     """Array namespace plus sparse kernels on the GPU (``backend.py:317-327``)."""
 
-    def __init__(self, device: str = "gpu", dtype=np.float64):
+    def __init__(self, device: str = "gpu", dtype=np.float64, autotune: bool = False):
         if device not in ("cpu", "gpu"):
             raise ValueError("device must be 'cpu' or 'gpu'")
         if device == "cpu":
@@ -40,6 +40,12 @@ class Backend:
         self.device = "gpu"
         self.dtype = np.dtype(dtype)
         self._tdtype = torch.float32 if self.dtype == np.float32 else torch.float64
+        # autotune: the first spmv on a matrix times the kernel's variants on
+        # it (pdlp_spmv_tune_*) and later calls use the fastest.  The choice is
+        # keyed by the matrix arrays' device addresses; a stale key costs only
+        # speed, since every variant computes the same product.
+        self.autotune = bool(autotune)
+        self._spmv_variant = {}
 
     # -- transfer ------------------------------------------------------------ #
 
@@ -76,9 +82,24 @@ class Backend:
     def spmv(self, rp, ri, rx, x, out, m):
         """``out = A x`` with ``A`` in CSR (``backend.py:373-384``)."""
         torch = _torch()
-        fn = self.lib.pdlp_spmv_f32 if rx.dtype == torch.float32 else self.lib.pdlp_spmv_f64
-        _lib.check(fn(int(m), rp.data_ptr(), ri.data_ptr(), rx.data_ptr(), x.data_ptr(),
-                      out.data_ptr(), self._stream()))
+        f32 = rx.dtype == torch.float32
+        if not self.autotune:
+            fn = self.lib.pdlp_spmv_f32 if f32 else self.lib.pdlp_spmv_f64
+            _lib.check(fn(int(m), rp.data_ptr(), ri.data_ptr(), rx.data_ptr(), x.data_ptr(),
+                          out.data_ptr(), self._stream()))
+            return out
+        key = (rp.data_ptr(), ri.data_ptr(), rx.data_ptr(), int(m), f32)
+        variant = self._spmv_variant.get(key)
+        if variant is None:
+            best = ctypes.c_int32(0)
+            tune = self.lib.pdlp_spmv_tune_f32 if f32 else self.lib.pdlp_spmv_tune_f64
+            _lib.check(tune(int(m), rp.data_ptr(), ri.data_ptr(), rx.data_ptr(), x.data_ptr(),
+                            out.data_ptr(), self._stream(), 10, ctypes.byref(best), None))
+            self._spmv_variant[key] = best.value
+            return out
+        fn = self.lib.pdlp_spmv_ex_f32 if f32 else self.lib.pdlp_spmv_ex_f64
+        _lib.check(fn(int(variant), int(m), rp.data_ptr(), ri.data_ptr(), rx.data_ptr(),
+                      x.data_ptr(), out.data_ptr(), self._stream()))
         return out
 
     def spmm(self, rp, ri, rx, X, out, m, k_batch):

@@ -47,17 +47,24 @@ int grid_1d(long long n, int per = kT) {
 // list order or the launch shape, and repeated calls give the same bits.
 constexpr int kSpmvWarps = 8;
 constexpr int kLongRow = 256;
-constexpr int kStageEntries = 512;     // entries a warp stages for one row block
+constexpr int kStageEntries = 256;     // entries a warp stages for one run of rows
 constexpr int kStageUnroll = 8;        // independent loads per lane in flight
 
-// The streamed block: entries [p0, p0 + cnt) of rows r0 .. r0 + nr - 1.
+// Variants of the row-block pass (pdlp_spmv_*_ex): streamed where a run of
+// rows fits the staging buffer, or the row-group path for every block.
+enum SpmvVariant : int { SPMV_AUTO = 0, SPMV_STREAMED = 1, SPMV_ROW_GROUPS = 2 };
+
+// Streams the rows i0 .. i1-1 of the warp's block (rows r0 + i), whose
+// entries are [p0, p0 + cnt), cnt <= kStageEntries: coalesced, independent
+// loads of indices and values, every gather at once, products staged in
+// shared memory; lane i then sums row i in storage order.
 template <typename T>
-__device__ __forceinline__ void spmv_block_staged(int r0, int nr, long long rs, long long re,
-                                                  long long p0, int cnt, int lane,
-                                                  const int* __restrict__ ri,
-                                                  const T* __restrict__ rx,
-                                                  const T* __restrict__ x, T* __restrict__ y,
-                                                  T* __restrict__ prod) {
+__device__ __forceinline__ void spmv_rows_staged(int r0, int i0, int i1, long long rs,
+                                                 long long re, long long p0, int cnt, int lane,
+                                                 const int* __restrict__ ri,
+                                                 const T* __restrict__ rx,
+                                                 const T* __restrict__ x, T* __restrict__ y,
+                                                 T* __restrict__ prod) {
   for (int q0 = 0; q0 < cnt; q0 += kStageUnroll * 32) {
     int idx[kStageUnroll];
     T val[kStageUnroll];
@@ -80,7 +87,7 @@ __device__ __forceinline__ void spmv_block_staged(int r0, int nr, long long rs, 
     }
   }
   __syncwarp();
-  if (lane < nr) {
+  if (lane >= i0 && lane < i1) {
     const int e = (int)(re - p0);
     int q = (int)(rs - p0);
     T a = T(0);
@@ -125,7 +132,7 @@ template <typename T>
 __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_rows32_kernel(
     int m, const int64_t* __restrict__ rp, const int* __restrict__ ri,
     const T* __restrict__ rx, const T* __restrict__ x, T* __restrict__ y,
-    int* __restrict__ long_rows) {
+    int* __restrict__ long_rows, int variant) {
   __shared__ T stage[kSpmvWarps][kStageEntries];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const long long nblk = ((long long)m + 31) / 32;
@@ -143,24 +150,41 @@ __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_rows32_kernel(
       if (slot < m) long_rows[2 + slot] = r0 + lane;
     }
     const unsigned long_mask = __ballot_sync(kAll, is_long);
-    const long long p0 = __shfl_sync(kAll, rs, 0);
-    const long long p1 = __shfl_sync(kAll, re, nr - 1);
-    if (long_mask == 0u && p1 - p0 <= kStageEntries) {
-      spmv_block_staged<T>(r0, nr, rs, re, p0, (int)(p1 - p0), lane, ri, rx, x, y, stage[w]);
-      continue;
+    const unsigned rows_mask = nr == 32 ? kAll : ((1u << nr) - 1u);
+    unsigned skip = long_mask;                  // rows the row-group path leaves alone
+    if (variant != SPMV_ROW_GROUPS) {
+      // the whole block, else each half of 16 rows, streamed when it has no
+      // long row and its entries fit the buffer
+      const long long pa = __shfl_sync(kAll, rs, 0), pb = __shfl_sync(kAll, re, nr - 1);
+      if (long_mask == 0u && pb - pa <= kStageEntries) {
+        spmv_rows_staged<T>(r0, 0, nr, rs, re, pa, (int)(pb - pa), lane, ri, rx, x, y, stage[w]);
+        continue;
+      }
+      for (int h = 0; h < 2 && 16 * h < nr; ++h) {
+        const int i0 = 16 * h, i1 = min(nr, i0 + 16);
+        const unsigned hb = (i1 - i0 == 16 ? 0xffffu : ((1u << (i1 - i0)) - 1u)) << i0;
+        const long long qa = __shfl_sync(kAll, rs, i0), qb = __shfl_sync(kAll, re, i1 - 1);
+        if ((long_mask & hb) == 0u && qb - qa <= kStageEntries) {
+          spmv_rows_staged<T>(r0, i0, i1, rs, re, qa, (int)(qb - qa), lane, ri, rx, x, y,
+                              stage[w]);
+          skip |= hb;
+        }
+      }
+      if ((skip & rows_mask) == rows_mask) continue;
     }
-    // mean length of the block's short rows -> lanes per row
-    long long len = (lane < nr && !is_long) ? re - rs : 0;
+    // mean length of the rows left -> lanes per row
+    const bool mine = lane < nr && !((skip >> lane) & 1u);
+    long long len = mine ? re - rs : 0;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) len += __shfl_xor_sync(kAll, len, off);
-    const int shorts = nr - __popc(long_mask);
-    const long long avg = shorts > 0 ? (len + shorts - 1) / shorts : 0;
-    if (avg <= 1) spmv_block_rows<T, 1>(r0, nr, rs, re, long_mask, lane, ri, rx, x, y);
-    else if (avg <= 2) spmv_block_rows<T, 2>(r0, nr, rs, re, long_mask, lane, ri, rx, x, y);
-    else if (avg <= 4) spmv_block_rows<T, 4>(r0, nr, rs, re, long_mask, lane, ri, rx, x, y);
-    else if (avg <= 8) spmv_block_rows<T, 8>(r0, nr, rs, re, long_mask, lane, ri, rx, x, y);
-    else if (avg <= 16) spmv_block_rows<T, 16>(r0, nr, rs, re, long_mask, lane, ri, rx, x, y);
-    else spmv_block_rows<T, 32>(r0, nr, rs, re, long_mask, lane, ri, rx, x, y);
+    const int left = __popc(rows_mask & ~skip);
+    const long long avg = left > 0 ? (len + left - 1) / left : 0;
+    if (avg <= 1) spmv_block_rows<T, 1>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
+    else if (avg <= 2) spmv_block_rows<T, 2>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
+    else if (avg <= 4) spmv_block_rows<T, 4>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
+    else if (avg <= 8) spmv_block_rows<T, 8>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
+    else if (avg <= 16) spmv_block_rows<T, 16>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
+    else spmv_block_rows<T, 32>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
   }
 }
 
@@ -247,8 +271,9 @@ int long_row_list(cudaStream_t st, size_t entries, int** out) {
 
 template <typename T>
 int launch_spmv(int m, const int64_t* rp, const int* ri, const T* rx, const T* x, T* y,
-                cudaStream_t st) {
+                cudaStream_t st, int variant = SPMV_AUTO) {
   if (m < 0) return fail(PDLP_ERR_ARG, "m must be >= 0");
+  if (variant < SPMV_AUTO || variant > SPMV_ROW_GROUPS) return fail(PDLP_ERR_ARG, "unknown SpMV variant");
   if (m == 0) return PDLP_OK;
   if (!rp || !ri || !rx || !x || !y) return fail(PDLP_ERR_ARG, "NULL pointer");
   int* long_rows = nullptr;
@@ -256,11 +281,47 @@ int launch_spmv(int m, const int64_t* rp, const int* ri, const T* rx, const T* x
   if (rc != PDLP_OK) return rc;
   const long long nblk = ((long long)m + 31) / 32;
   const int g = (int)std::min((nblk + kSpmvWarps - 1) / kSpmvWarps, 1LL << 30);
-  spmv_rows32_kernel<T><<<g, kSpmvWarps * 32, 0, st>>>(m, rp, ri, rx, x, y, long_rows);
+  spmv_rows32_kernel<T><<<g, kSpmvWarps * 32, 0, st>>>(m, rp, ri, rx, x, y, long_rows, variant);
   spmv_long_rows_kernel<T><<<592, kSpmvWarps * 32, 0, st>>>(rp, ri, rx, x, y, m, long_rows);
   count_launches(2);
   PDLP_CUDA(cudaGetLastError());
   return PDLP_OK;
+}
+
+// The SpMV autotuner: times every variant of the row-block pass on the
+// caller's matrix and vectors (one warm call each, then `reps` calls bracketed
+// by CUDA events on the caller's stream) and returns the fastest.  Its cost is
+// a few dozen SpMVs; the caller keeps the choice for the matrix.
+template <typename T>
+int tune_spmv(int m, const int64_t* rp, const int* ri, const T* rx, const T* x, T* y,
+              cudaStream_t st, int reps, int* best, double* ms_out) {
+  if (!best) return fail(PDLP_ERR_ARG, "best is NULL");
+  if (reps <= 0) reps = 10;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  PDLP_CUDA(cudaEventCreate(&e0));
+  const cudaError_t ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) { cudaEventDestroy(e0); return cuda_fail(ce, "cudaEventCreate"); }
+  const int variants[2] = {SPMV_STREAMED, SPMV_ROW_GROUPS};
+  double best_ms = 0.0;
+  int rc = PDLP_OK;
+  *best = SPMV_STREAMED;
+  for (int k = 0; k < 2 && rc == PDLP_OK; ++k) {
+    rc = launch_spmv<T>(m, rp, ri, rx, x, y, st, variants[k]);
+    if (rc != PDLP_OK) break;
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < reps && rc == PDLP_OK; ++r) rc = launch_spmv<T>(m, rp, ri, rx, x, y, st, variants[k]);
+    cudaEventRecord(e1, st);
+    const cudaError_t se = cudaEventSynchronize(e1);
+    if (se != cudaSuccess) { rc = cuda_fail(se, "cudaEventSynchronize"); break; }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    const double per = (double)ms / reps;
+    if (ms_out) ms_out[k] = per;
+    if (k == 0 || per < best_ms) { best_ms = per; *best = variants[k]; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
 }
 
 // Y = A X, X row-major (ncols, k): one thread per (row, column of X); the
@@ -476,6 +537,30 @@ int pdlp_spmv_f64(int32_t m, const int64_t* rp, const int32_t* ri, const double*
 int pdlp_spmv_f32(int32_t m, const int64_t* rp, const int32_t* ri, const float* rx,
                   const float* x, float* y, void* stream) {
   return launch_spmv<float>(m, rp, ri, rx, x, y, (cudaStream_t)stream);
+}
+
+int pdlp_spmv_ex_f64(int32_t variant, int32_t m, const int64_t* rp, const int32_t* ri,
+                     const double* rx, const double* x, double* y, void* stream) {
+  return launch_spmv<double>(m, rp, ri, rx, x, y, (cudaStream_t)stream, variant);
+}
+
+int pdlp_spmv_ex_f32(int32_t variant, int32_t m, const int64_t* rp, const int32_t* ri,
+                     const float* rx, const float* x, float* y, void* stream) {
+  return launch_spmv<float>(m, rp, ri, rx, x, y, (cudaStream_t)stream, variant);
+}
+
+int pdlp_spmv_tune_f64(int32_t m, const int64_t* rp, const int32_t* ri, const double* rx,
+                       const double* x, double* y, void* stream, int32_t reps,
+                       int32_t* best_variant, double* ms_per_variant) {
+  return tune_spmv<double>(m, rp, ri, rx, x, y, (cudaStream_t)stream, reps, best_variant,
+                           ms_per_variant);
+}
+
+int pdlp_spmv_tune_f32(int32_t m, const int64_t* rp, const int32_t* ri, const float* rx,
+                       const float* x, float* y, void* stream, int32_t reps,
+                       int32_t* best_variant, double* ms_per_variant) {
+  return tune_spmv<float>(m, rp, ri, rx, x, y, (cudaStream_t)stream, reps, best_variant,
+                          ms_per_variant);
 }
 
 int pdlp_spmm_f64(int32_t m, int32_t k, const int64_t* rp, const int32_t* ri,

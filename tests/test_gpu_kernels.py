@@ -99,6 +99,80 @@ def test_spmv_long_rows_and_partial_row_blocks(bk):
     np.testing.assert_allclose(out32.cpu().numpy(), exp, rtol=1e-4, atol=1e-3)
 
 
+def _spmv_ex(bk, variant, A, x, poison=12345.0, f32=False):
+    import ctypes
+    import torch
+    from sovereign_moe_b200 import _lib
+    dt = torch.float32 if f32 else torch.float64
+    rp, ri = bk.pointer(A.rp), bk.index(A.ri)
+    rx = bk.to_device(A.rx).to(dt)
+    xd = bk.to_device(x).to(dt)
+    out = torch.full((A.m,), poison, dtype=dt, device="cuda")
+    fn = bk.lib.pdlp_spmv_ex_f32 if f32 else bk.lib.pdlp_spmv_ex_f64
+    _lib.check(fn(variant, A.m, rp.data_ptr(), ri.data_ptr(), rx.data_ptr(), xd.data_ptr(),
+                  out.data_ptr(), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    bk.sync()
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+def test_spmv_variants_match_oracle(bk, variant):
+    """Both row-block variants (streamed runs of rows, row groups) on rows of
+    every length class: empty, short, up to the staging buffer, long (the
+    second launch), mixed within one 32-row block and its 16-row halves."""
+    rng = np.random.default_rng(40 + variant)
+    lens = rng.choice([0, 1, 3, 7, 8, 9, 15, 16, 17, 40, 100, 255, 256, 257, 600], size=203)
+    m, n = len(lens), 2000
+    rows = np.repeat(np.arange(m), lens)
+    cols = np.concatenate([rng.choice(n, size=k, replace=False) for k in lens])
+    A = SparseMatrix.from_triplets(rows, cols, rng.standard_normal(rows.size), m, n)
+    x = rng.standard_normal(n)
+    exp = po.spmv(A.rp, A.ri, A.rx, x)
+    np.testing.assert_allclose(_spmv_ex(bk, variant, A, x), exp, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(_spmv_ex(bk, variant, A, x, f32=True), exp, rtol=1e-4, atol=1e-3)
+
+
+def test_streamed_rows_equal_oracle_bitwise(bk):
+    """Rows of at most 16 entries are always streamed (every 16-row half fits
+    the 256-entry buffer), and a streamed row is the oracle's storage-order
+    sum of rounded products, bit for bit."""
+    A, rng = _random_csr(5000, 3000, 4, seed=9)          # about 2.4 entries per row
+    lens = np.diff(A.rp)
+    assert lens.max() <= 16
+    x = rng.standard_normal(A.n)
+    got = _spmv_ex(bk, 1, A, x)
+    assert np.array_equal(got, po.spmv(A.rp, A.ri, A.rx, x))
+
+
+def test_spmv_tuner_and_autotuned_backend(bk):
+    import ctypes
+    import torch
+    from sovereign_moe_b200 import _lib
+    from sovereign_moe_b200.backend import Backend
+    A, rng = _random_csr(4000, 9000, 6, seed=12)
+    x = rng.standard_normal(A.n)
+    exp = po.spmv(A.rp, A.ri, A.rx, x)
+    rp, ri, rx, xd = bk.pointer(A.rp), bk.index(A.ri), bk.to_device(A.rx), bk.to_device(x)
+    out = bk.zeros(A.m) + 12345.0
+    best = ctypes.c_int32(-1)
+    ms = (ctypes.c_double * 2)()
+    _lib.check(bk.lib.pdlp_spmv_tune_f64(A.m, rp.data_ptr(), ri.data_ptr(), rx.data_ptr(),
+                                         xd.data_ptr(), out.data_ptr(),
+                                         ctypes.c_void_p(torch.cuda.current_stream().cuda_stream),
+                                         5, ctypes.byref(best), ms))
+    assert best.value in (_lib.PDLP_SPMV_STREAMED, _lib.PDLP_SPMV_ROW_GROUPS)
+    assert ms[0] > 0 and ms[1] > 0
+    assert ms[best.value - 1] == min(ms[0], ms[1])
+    np.testing.assert_allclose(out.cpu().numpy(), exp, rtol=1e-12, atol=1e-12)
+    tuned = Backend("gpu", autotune=True)
+    for _ in range(2):                                   # tunes, then uses the choice
+        o = tuned.zeros(A.m) + 12345.0
+        tuned.spmv(rp, ri, rx, xd, o, A.m)
+        tuned.sync()
+        np.testing.assert_allclose(o.cpu().numpy(), exp, rtol=1e-12, atol=1e-12)
+    assert len(tuned._spmv_variant) == 1
+
+
 @pytest.mark.parametrize("k", [1, 8, 32, 33, 64])
 def test_spmm_matches_oracle(bk, k):
     A, rng = _random_csr(300, 500, 4, seed=k)

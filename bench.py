@@ -275,6 +275,10 @@ class GpuArm:
         self.host_arrays = ((_lib.ProblemDesc * n)(*[d for _, d in self.host]),
                             (_lib.Params * n)(*self.hparams))
         self.single = BatchEngine(max_slots=1)
+        # the team planner's iteration estimates, learned from the LPs of the
+        # earlier steps (per columns-per-row class; results do not depend on them)
+        from sovereign_moe_b200.schedule import IterationModel
+        self.model = IterationModel()
         self.latencies = []
         self.engine_ms = 0.0
         self.engine_bytes = 0.0
@@ -292,6 +296,8 @@ class GpuArm:
         outs = self.out_host if host else self.out_dev
         mem = L.PDLP_MEM_HOST if host else L.PDLP_MEM_DEVICE
         darr, parr = (self.host_arrays if host else self.dev_arrays)
+        for i, k in enumerate(self.lps):
+            parr[i].expected_iterations = self.model.predict(k.problem)
         t0 = time.perf_counter()
         slot_arr = (ct.c_int32 * len(descs))()
         L.check(c.pdlp_batch_admit_many(self.eng.h, len(descs), darr, parr, slot_arr, None))
@@ -313,6 +319,7 @@ class GpuArm:
             statuses.append(r.status)
             starts.append(r.device_start_ns)
             ends.append(r.device_end_ns)
+            self.model.observe(k.problem, int(r.iterations))
             self.per_lp.append({"m": int(k.problem.A.m), "n": int(k.problem.A.n),
                                 "nnz": int(k.problem.A.nnz), "iterations": int(r.iterations),
                                 "restarts": int(r.restarts), "start_ns": int(r.device_start_ns),
@@ -522,7 +529,10 @@ def run_gpu(args, rank, world):
                        "nnz_per_col": "4-12", "total_nnz": int(total_nnz),
                        "tolerance": "rel KKT 1e-6 (eps_abs=eps_rel=1e-6, feas_cap=1e-6)",
                        "l2": "inputs larger than L2 (>126 MB of matrix data per step)",
-                       "parallelism": f"replicas x{world}", "worst_rel_obj_err": worst},
+                       "parallelism": f"replicas x{world}", "worst_rel_obj_err": worst,
+                       "scheduling": ("block teams sized by expected remaining iterations: "
+                                      "median iterations per columns-per-row class, learned "
+                                      "from the LPs finished in earlier steps")},
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -669,7 +679,8 @@ def run_spmv(args):
     mats.append((f"power_law_{int(1e6 * sc)}x{int(3e6 * sc)}",
                  power_law(seed=0, m=int(1_000_000 * sc), n=int(3_000_000 * sc),
                            nnz=int(10_000_000 * sc)).problem))
-    names = {_lib.PDLP_SPMV_STREAMED: "streamed", _lib.PDLP_SPMV_ROW_GROUPS: "row_groups"}
+    names = {_lib.PDLP_SPMV_STREAMED: "streamed", _lib.PDLP_SPMV_ROW_GROUPS: "row_groups",
+             _lib.PDLP_SPMV_BANDED: "banded"}
     rows = []
     for name, prob in mats:
         A = prob.A
@@ -707,14 +718,15 @@ def run_spmv(args):
 
                 per = {names[v]: timed(v) for v in names}
                 best = ctypes.c_int32(0)
-                tms = (ctypes.c_double * 2)()
+                tms = (ctypes.c_double * 3)()
                 _lib.check(tune(int(r), rp.data_ptr(), ri.data_ptr(), rx.data_ptr(), x.data_ptr(),
                                 y.data_ptr(), stream.cuda_stream, 10, ctypes.byref(best), tms))
                 ms = per[names[best.value]]
                 rows.append({"matrix": name, "product": side, "dtype": prec, "rows": int(r),
                              "nnz": nnz, "algorithmic_bytes": algo,
                              "ms_per_variant": per, "tuned_variant": names[best.value],
-                             "tuner_ms_warm_l2": {"streamed": tms[0], "row_groups": tms[1]},
+                             "tuner_ms_warm_l2": {"streamed": tms[0], "row_groups": tms[1],
+                                                  "banded": tms[2]},
                              "ms": ms, "GBps": algo / ms / 1e6,
                              "frac_of_measured_hbm": algo / ms / 1e6 / peak})
                 del rp, ri, rx, x, y
@@ -834,6 +846,51 @@ def run_bnr(args):
     return 0
 
 
+def run_tune(args):
+    """The engine autotuner on the headline batch (256 uneven LPs): tune one
+    LP per nnz profile (``sovereign_moe_b200.tuning.tune``), then solve the
+    batch with the engine's fixed rules and with the tuned choices, each
+    device-resident like the headline ``value`` (3 warm-up batches, then
+    ``--steps`` timed ones), and report both rates and the tuning cost."""
+    import torch
+    from sovereign_moe_b200 import tuning
+    from sovereign_moe_b200.batch import BatchEngine
+    lps = make_batch(seed=1000)
+    probs = [k.problem for k in lps]
+    tuning.clear()
+    t0 = time.perf_counter()
+    done = tuning.tune(probs, params())
+    tune_s = time.perf_counter() - t0
+    out = {}
+    for mode in ("fixed", "tuned"):
+        with BatchEngine(max_slots=len(probs), autotune=(mode == "tuned")) as eng:
+            for _ in range(3):
+                eng.solve_all(probs, params())
+            e0, e1 = _sync_events(torch)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(args.steps):
+                sols = eng.solve_all(probs, params())
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / args.steps
+        worst = max(abs(s.objective - k.f_star) / max(1.0, abs(k.f_star))
+                    for s, k in zip(sols, lps))
+        out[mode] = {"solves_per_s": len(probs) / (ms / 1000.0), "ms_per_batch": ms,
+                     "worst_rel_obj_err": worst}
+    gains = [v["default_us_per_iteration"] / v["us_per_iteration"] for v in done.values()]
+    print(json.dumps({"metric": "autotuned engine: LP solves/s at rel KKT 1e-6",
+                      "unit": "solves/s", "fixed": out["fixed"], "tuned": out["tuned"],
+                      "ratio_tuned_over_fixed": out["tuned"]["solves_per_s"] / out["fixed"]["solves_per_s"],
+                      "profiles_tuned": len(done), "tuning_s": tune_s,
+                      "solo_gain_per_profile": {"min": min(gains), "median": statistics.median(gains),
+                                                "max": max(gains)},
+                      "choices": [{"key": list(k), **v} for k, v in done.items()],
+                      "config": {"workload": WORKLOAD, "lps": len(probs)}}), flush=True)
+    tuning.clear()
+    return 0
+
+
 def run_precision(args):
     """FP32-SpMV against float64 per instance: config-1-shaped known-optimum
     LPs (230 x 2025, seeds 0-7) and 8 LPs of the uneven batch, each solved at
@@ -902,7 +959,7 @@ def main():
                     help="skip the one-at-a-time pass through the public solve_pdlp")
     ap.add_argument("--workload", default="batch",
                     choices=["batch", "blend", "powerlaw", "serving", "engine-steps", "spmv",
-                             "precision", "bnr"],
+                             "precision", "bnr", "tune"],
                     help="batch: the headline metric; the others print auxiliary lines")
     ap.add_argument("--iters", type=int, default=2000)
     ap.add_argument("--scale", type=float, default=1.0)
@@ -926,6 +983,8 @@ def main():
         return run_precision(args)
     if args.workload == "bnr":
         return run_bnr(args)
+    if args.workload == "tune":
+        return run_tune(args)
     if args.warmup < 3 and args.impl == "ours":
         ap.error("--warmup must be >= 3")
     rank = int(os.environ.get("RANK", "0"))

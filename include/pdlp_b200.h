@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PDLP_ABI_VERSION 3
+#define PDLP_ABI_VERSION 4
 
 /* ---- error codes ------------------------------------------------------- */
 #define PDLP_OK                   0
@@ -116,6 +116,14 @@ typedef struct pdlp_params {
      * eps_infeasible times the ray's objective.  Off by default. */
     int32_t detect_infeasibility;
     double eps_infeasible;              /* default 1e-8                      */
+    /* Scheduling hint (no counterpart in the reference): the caller's
+     * estimate of the PDHG iterations this LP needs, 0 = none.  When every
+     * running LP of a batch has one, the engine sizes their block teams by
+     * expected remaining work (work per iteration times the iterations left)
+     * instead of work per iteration, so that the LPs expected to run longest
+     * get their blocks first.  Results do not depend on it: an LP's bits are
+     * the same whichever warps run its tiles. */
+    double expected_iterations;
 } pdlp_params;
 
 void pdlp_params_default(pdlp_params* p);
@@ -179,6 +187,12 @@ typedef struct pdlp_batch_config {
                                    A wait that runs out ends the step with
                                    PDLP_ERR_BARRIER_TIMEOUT and the batch
                                    refuses later calls (PDLP_ERR_STATE)     */
+    int32_t autotune;           /* 1: an admitted LP whose nnz profile has an
+                                   entry in the process's tuning cache
+                                   (pdlp_tune_lp) takes its lanes per row and
+                                   tile shape from it; 0: the engine's fixed
+                                   rules (lanes from the mean row length,
+                                   tiles tile_rows x tile_nnz)             */
     int32_t test_withhold_arrival; /* test hook, 0 = off.  1: the last block
                                    of the first team of two or more blocks
                                    leaves the kernel at its first barrier
@@ -245,6 +259,52 @@ int64_t pdlp_slot_bytes(int32_t m, int32_t n, int64_t nnz);
 int pdlp_batch_last_timing(pdlp_batch* b, double* ms, double* iter_bytes,
                            int64_t* iterations);
 
+/* ---- engine autotuner --------------------------------------------------- *
+ * No counterpart in the reference, whose kernels have one fixed launch shape
+ * (backend.py:379-384).  The tuner picks, per nnz profile, the lanes that sum
+ * each row of the A pass and of the A^T pass and the tile shape (rows and
+ * entries per warp tile), by timing short solo runs of an LP with each
+ * candidate: lanes 1, 2, 4 for either pass with the default tiles, then tiles
+ * of 64 or 32 rows and 512 or 256 entries with the best lanes.  Each run
+ * admits the LP into a private one-slot batch on `stream`, runs it past its
+ * preconditioning, then times 2 x 64 engine steps (the faster counts), so a
+ * tuning costs about a dozen short solves.  Every candidate runs on the same
+ * number of blocks, about eight default tiles per warp: the load a warp
+ * carries in a full batch (alone on all the blocks it can use, an LP would
+ * favour small tiles, which lose in a loaded batch).  Results go to a process-wide
+ * cache (guarded by a mutex) keyed by the LP's profile: batches created with
+ * pdlp_batch_config.autotune = 1 use it at admission.  Tuning changes only
+ * how an LP's rows are split across lanes and warps, so a tuned LP's result
+ * equals the untuned one up to the summation order. */
+typedef struct pdlp_tune_key {
+    int32_t rows_bucket;        /* floor(log2(m + 1))                       */
+    int32_t row_len_bucket;     /* floor(2 log2(nnz / m + 1)): half octaves  */
+    int32_t col_len_bucket;     /* floor(2 log2(nnz / n + 1))               */
+} pdlp_tune_key;
+
+typedef struct pdlp_tuning {
+    int32_t lanes_rows, lanes_cols;     /* lanes per row: A pass, A^T pass   */
+    int32_t tile_rows, tile_nnz;        /* warp tile: rows and entries       */
+    double us_per_iteration;            /* the choice's time per PDHG
+                                           iteration of the tuned LP, on the
+                                           tuner's fixed block count        */
+    double default_us_per_iteration;    /* the same with the fixed rules     */
+} pdlp_tuning;
+
+void pdlp_tune_key_of(int32_t m, int32_t n, int64_t nnz, pdlp_tune_key* key);
+/* Tunes the engine for this LP (host or device arrays, as for admission) and
+ * stores the result under its profile; *out (optional) receives it. */
+int pdlp_tune_lp(const pdlp_problem_desc* prob, const pdlp_params* params, void* stream,
+                 pdlp_tuning* out);
+int pdlp_tune_cache_size(void);
+/* Entry i (0 <= i < size) of the cache, in key order. */
+int pdlp_tune_cache_get(int32_t i, pdlp_tune_key* key, pdlp_tuning* tuning);
+/* Stores an entry (e.g. one saved by an earlier process); the choice is
+ * checked: lanes 1, 2, 4, 8, 16 or 32, 1 <= tile_rows <= 64,
+ * 1 <= tile_nnz <= 512. */
+int pdlp_tune_cache_put(const pdlp_tune_key* key, const pdlp_tuning* tuning);
+void pdlp_tune_cache_clear(void);
+
 /* ---- kernel-level Backend (backend.py:317-493) -------------------------- *
  * Device pointers; `stream` as above.  FP64 unless named _f32. */
 
@@ -264,10 +324,15 @@ int pdlp_spmv_f32(int32_t m, const int64_t* rp, const int32_t* ri, const float* 
  * staged in shared memory and each row summed in storage order; other rows
  * take the row-group path.  ROW_GROUPS: every row takes the row-group path
  * (L lanes per row from the block's mean row length, strided sums then a
- * xor butterfly).  Both give the same results up to the summation order. */
+ * xor butterfly).  BANDED: as STREAMED, but a block of 256 rows whose
+ * streamed entries' column indices span at most 3072 columns first loads x
+ * over that span into shared memory, and gathers from it (banded matrices,
+ * e.g. multi-period plans).  All give the same results up to the summation
+ * order; STREAMED and BANDED sum each streamed row in storage order. */
 #define PDLP_SPMV_AUTO        0
 #define PDLP_SPMV_STREAMED    1
 #define PDLP_SPMV_ROW_GROUPS  2
+#define PDLP_SPMV_BANDED      3
 int pdlp_spmv_ex_f64(int32_t variant, int32_t m, const int64_t* rp, const int32_t* ri,
                      const double* rx, const double* x, double* y, void* stream);
 int pdlp_spmv_ex_f32(int32_t variant, int32_t m, const int64_t* rp, const int32_t* ri,
@@ -275,8 +340,8 @@ int pdlp_spmv_ex_f32(int32_t variant, int32_t m, const int64_t* rp, const int32_
 /* The SpMV autotuner: times each variant on this matrix and these vectors
  * (one warm call, then `reps` calls, 0 = 10, with CUDA events on `stream`),
  * writes y = A x, and returns the fastest variant in *best_variant and each
- * variant's milliseconds per call in ms_per_variant[2] (STREAMED, ROW_GROUPS;
- * optional).  Synchronises the stream.  The reference has a fixed launch
+ * variant's milliseconds per call in ms_per_variant[3] (STREAMED, ROW_GROUPS,
+ * BANDED; optional).  Synchronises the stream.  The reference has a fixed launch
  * shape (backend.py:379-384); the caller keeps the choice per matrix. */
 int pdlp_spmv_tune_f64(int32_t m, const int64_t* rp, const int32_t* ri, const double* rx,
                        const double* x, double* y, void* stream, int32_t reps,

@@ -28,6 +28,7 @@ PDLP_MEM_HOST = 1
 PDLP_SPMV_AUTO = 0
 PDLP_SPMV_STREAMED = 1
 PDLP_SPMV_ROW_GROUPS = 2
+PDLP_SPMV_BANDED = 3
 
 PDLP_STATUS_RUNNING = -1
 PDLP_SLOT_FREE = -2
@@ -57,7 +58,8 @@ class Params(ctypes.Structure):
                 ("primal_weight_smoothing", ctypes.c_double), ("scaling", ctypes.c_int32),
                 ("power_start", _c_p), ("time_used", ctypes.c_double),
                 ("history_capacity", ctypes.c_int32), ("precision", ctypes.c_int32),
-                ("detect_infeasibility", ctypes.c_int32), ("eps_infeasible", ctypes.c_double)]
+                ("detect_infeasibility", ctypes.c_int32), ("eps_infeasible", ctypes.c_double),
+                ("expected_iterations", ctypes.c_double)]
 
 
 class Result(ctypes.Structure):
@@ -77,7 +79,19 @@ class BatchConfig(ctypes.Structure):
                 ("block_threads", ctypes.c_int32), ("tile_rows", ctypes.c_int32),
                 ("tile_nnz", ctypes.c_int32), ("lanes_override", ctypes.c_int32),
                 ("memory_budget", ctypes.c_int64), ("barrier_timeout_us", ctypes.c_int64),
-                ("test_withhold_arrival", ctypes.c_int32)]
+                ("autotune", ctypes.c_int32), ("test_withhold_arrival", ctypes.c_int32)]
+
+
+class TuneKey(ctypes.Structure):
+    _fields_ = [("rows_bucket", ctypes.c_int32), ("row_len_bucket", ctypes.c_int32),
+                ("col_len_bucket", ctypes.c_int32)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("lanes_rows", ctypes.c_int32), ("lanes_cols", ctypes.c_int32),
+                ("tile_rows", ctypes.c_int32), ("tile_nnz", ctypes.c_int32),
+                ("us_per_iteration", ctypes.c_double),
+                ("default_us_per_iteration", ctypes.c_double)]
 
 
 # Every symbol include/pdlp_b200.h declares, with its argument types.
@@ -130,6 +144,14 @@ SIGNATURES = {
                               _c_p, _c_p, _i32], ctypes.c_int),
     "pdlp_bnr_step_sizes": ([_c_p, _i32, _c_p, _c_p], ctypes.c_int),
     "pdlp_dot_noalloc": ([_i64, _c_p, _c_p, ctypes.POINTER(_d), _c_p], ctypes.c_int),
+    "pdlp_tune_key_of": ([_i32, _i32, _i64, ctypes.POINTER(TuneKey)], None),
+    "pdlp_tune_lp": ([ctypes.POINTER(ProblemDesc), ctypes.POINTER(Params), _c_p,
+                      ctypes.POINTER(Tuning)], ctypes.c_int),
+    "pdlp_tune_cache_size": ([], ctypes.c_int),
+    "pdlp_tune_cache_get": ([_i32, ctypes.POINTER(TuneKey), ctypes.POINTER(Tuning)],
+                            ctypes.c_int),
+    "pdlp_tune_cache_put": ([ctypes.POINTER(TuneKey), ctypes.POINTER(Tuning)], ctypes.c_int),
+    "pdlp_tune_cache_clear": ([], None),
 }
 
 _LIB = None

@@ -31,7 +31,7 @@ class BatchEngine:
 
     def __init__(self, max_slots=256, persistent=True, tile_rows=0, tile_nnz=0,
                  lanes_override=0, memory_budget=0, stream=None, barrier_timeout_us=0,
-                 test_withhold_arrival=False):
+                 autotune=False, test_withhold_arrival=False):
         self.lib = _lib.load()
         cfg = _lib.BatchConfig()
         self.lib.pdlp_batch_config_default(ctypes.byref(cfg))
@@ -44,6 +44,7 @@ class BatchEngine:
         cfg.lanes_override = int(lanes_override)
         cfg.memory_budget = int(memory_budget)
         cfg.barrier_timeout_us = int(barrier_timeout_us)
+        cfg.autotune = 1 if autotune else 0
         cfg.test_withhold_arrival = 1 if test_withhold_arrival else 0
         h = ctypes.c_void_p()
         code = self.lib.pdlp_batch_create(ctypes.byref(cfg), stream, ctypes.byref(h))
@@ -73,14 +74,18 @@ class BatchEngine:
 
     # -- slots ------------------------------------------------------------- #
 
-    def admit(self, prob, params: PDLPParams | None = None, power_start="reference"):
+    def admit(self, prob, params: PDLPParams | None = None, power_start="reference", hint=0.0):
         """Copy ``prob`` to the device and precondition it; returns the slot.
-        Raises ``PDLPError`` with code ``PDLP_ERR_OOM`` when it does not fit."""
+        ``hint``: the LP's expected iterations (0 = none), the engine's
+        team-sizing hint.  Raises ``PDLPError`` with code ``PDLP_ERR_OOM``
+        when it does not fit."""
         params = params or PDLPParams()
         _check_device(params.device)
         t0 = time.perf_counter()
         desc, keep = problem_desc(prob)
         p, keep_v0 = params_struct(params, int(prob.A.n), power_start=power_start)
+        if hint:
+            p.expected_iterations = float(hint)
         slot = ctypes.c_int32(-1)
         _lib.check(self.lib.pdlp_batch_admit(self.h, ctypes.byref(desc), ctypes.byref(p),
                                              ctypes.byref(slot)))
@@ -88,11 +93,13 @@ class BatchEngine:
         self._meta[slot.value] = (prob, params, int(p.history_capacity), t0)
         return slot.value
 
-    def admit_many(self, probs, params: PDLPParams | None = None, power_start="reference"):
+    def admit_many(self, probs, params: PDLPParams | None = None, power_start="reference",
+                   hints=None):
         """Admit several LPs with three host synchronisations in all (instead
-        of two per LP).  Returns ``(slots, codes)``: the slot of each LP (-1
-        when refused) and its return code; a refused LP does not stop the
-        others."""
+        of two per LP).  ``hints`` (optional): each LP's expected iterations,
+        the engine's team-sizing hint.  Returns ``(slots, codes)``: the slot of
+        each LP (-1 when refused) and its return code; a refused LP does not
+        stop the others."""
         params = params or PDLPParams()
         _check_device(params.device)
         count = len(probs)
@@ -105,6 +112,8 @@ class BatchEngine:
         for i, prob in enumerate(probs):
             d, k = problem_desc(prob)
             p, kv = params_struct(params, int(prob.A.n), power_start=power_start)
+            if hints is not None:
+                p.expected_iterations = float(hints[i])
             descs[i], prms[i] = d, p
             keep.append((k, kv))
         slots = np.full(count, -1, dtype=np.int32)
@@ -181,9 +190,9 @@ class BatchEngine:
     def slot_bytes(self, m, n, nnz):
         return int(self.lib.pdlp_slot_bytes(int(m), int(n), int(nnz)))
 
-    def solve_all(self, probs, params=None):
+    def solve_all(self, probs, params=None, hints=None):
         """Admit every LP, run to completion, fetch and retire: list of Solutions."""
-        slots, codes = self.admit_many(probs, params)
+        slots, codes = self.admit_many(probs, params, hints=hints)
         for c in codes:
             _lib.check(c)
         self.run()

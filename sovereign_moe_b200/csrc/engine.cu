@@ -5,6 +5,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -131,6 +132,7 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
       for (int t = r0; t < r1; ++t) {
         const Tile cur = next;
         if (t + 1 < r1) next = A.rtiles[t + 1];      // prefetch the next descriptor
+        ph.flush = t + 1 >= r1 || next.group != cur.group;
         process_rtile(A, cur, t, W, lane, pc, ph);
       }
     }
@@ -149,6 +151,7 @@ __global__ void __launch_bounds__(kBlock, 4) engine_persistent(EngineArgs A) {
       for (int t = c0; t < c1; ++t) {
         const Tile cur = next;
         if (t + 1 < c1) next = A.ctiles[t + 1];
+        ph.flush = t + 1 >= c1 || next.group != cur.group;
         process_ctile(A, cur, t, W, lane, pc, ph);
       }
     }
@@ -459,6 +462,7 @@ struct Slot {
   std::vector<Tile> rt, ct;   // tiles with local ranges (inst field = slot)
   std::vector<double> rtw, ctw;   // work estimate per tile
   double bytes_per_iter = 0.0;
+  double expected_iters = 0.0;    // the caller's scheduling hint (0: none)
 };
 
 }  // namespace
@@ -518,6 +522,9 @@ struct pdlp_batch {
   State* h_init = nullptr;             // pinned: initial states, one per slot
   int64_t* h_ptrs = nullptr;           // pinned: device pointer arrays read for admission
   size_t cap_hptrs = 0;
+  bool force_set = false;              // tuning runs: every admission takes `force`
+  pdlp_tuning force{};
+  int force_blocks = 0;                // tuning runs: the one team's block count (0: free)
   int withhold_candidate = -1;         // last block of the first multi-block team
 };
 
@@ -636,12 +643,18 @@ static void make_groups(std::vector<Tile>& tiles, int t0, int t1, int group_base
 
 // The block teams of a persistent launch.  With many running instances one
 // team of blocks steps them all.  With fewer (at most kTeamsFrom), each
-// instance gets its own team, sized by its share of the work and its tile
-// count, so that no instance waits at a barrier for another's tiles.  On the
-// 256-LP batch (engine time per batch, with the idle rule of the kernel),
-// teams from 160, 200 and 256 running instances measured 585, 571 and 541 ms.
-// Returns the blocks of each running instance's team, in `run` order, or
-// nothing for one team.
+// instance gets its own team, so that no instance waits at a barrier for
+// another's tiles.  Teams get blocks in proportion to each instance's weight,
+// but never more than one tile per warp can use: the blocks an instance
+// cannot use go to the others (water-filling), and the blocks left by
+// rounding go to the largest remainders.  The weight is the instance's work
+// per iteration, times its expected remaining iterations when every running
+// instance carries an estimate (pdlp_params.expected_iterations): an
+// instance past its estimate is taken to need half as many iterations again.
+// On the 256-LP batch (engine time per batch, with the idle rule of the
+// kernel), teams from 160, 200 and 256 running instances measured 585, 571
+// and 541 ms.  Returns the blocks of each running instance's team, in `run`
+// order, or nothing for one team.
 static std::vector<int> plan_teams(const pdlp_batch* b, const std::vector<int>& run,
                                    int max_blocks) {
   constexpr int kTeamsFrom = 256;
@@ -649,25 +662,68 @@ static std::vector<int> plan_teams(const pdlp_batch* b, const std::vector<int>& 
   if (!b->cfg.persistent || run.size() < 2 ||
       (int)run.size() > std::min(kTeamsFrom, kMaxTeams) || (int)run.size() > max_blocks)
     return tblocks;
-  double total = 0.0;
-  std::vector<double> w(run.size());
-  std::vector<int> want(run.size());
-  for (size_t k = 0; k < run.size(); ++k) {
+  const size_t T = run.size();
+  bool hinted = true;
+  for (int s : run) hinted = hinted && b->slots[s].expected_iters > 0.0;
+  std::vector<double> w(T);
+  std::vector<int> want(T);
+  for (size_t k = 0; k < T; ++k) {
     const Slot& sl = b->slots[run[k]];
-    for (double v : sl.rtw) w[k] += v;
-    for (double v : sl.ctw) w[k] += v;
-    total += w[k];
+    double per = 0.0;
+    for (double v : sl.rtw) per += v;
+    for (double v : sl.ctw) per += v;
+    if (hinted) {
+      const double e = sl.expected_iters, d = (double)b->iters_before[run[k]];
+      const double left = d < e ? e - d : 0.5 * d;
+      per *= std::max(left, 0.1 * e);
+    }
+    w[k] = per;
     const int tiles = std::max(sl.inst.rt_end - sl.inst.rt_begin, sl.inst.ct_end - sl.inst.ct_begin);
     want[k] = std::max(1, (tiles + kWarps - 1) / kWarps);    // one tile per warp
   }
-  tblocks.resize(run.size());
+  tblocks.assign(T, 0);
+  std::vector<char> full(T, 0);
+  double wfree = 0.0;
+  for (size_t k = 0; k < T; ++k) wfree += w[k];
+  int free_blocks = max_blocks;
+  size_t nfree = T;
+  for (bool again = true; again && nfree > 0;) {
+    again = false;
+    const double wf = wfree;
+    const int fb = free_blocks;
+    const size_t nf = nfree;
+    for (size_t k = 0; k < T; ++k) {
+      if (full[k]) continue;
+      const double share = wf > 0.0 ? fb * (w[k] / wf) : (double)fb / nf;
+      if (share >= want[k]) {           // more than it can use: all it can use
+        full[k] = 1;
+        tblocks[k] = want[k];
+        free_blocks -= want[k];
+        wfree -= w[k];
+        --nfree;
+        again = true;
+      }
+    }
+  }
+  std::vector<std::pair<double, int>> frac;
   int used = 0;
-  for (size_t k = 0; k < run.size(); ++k) {
-    const int share = (int)((double)max_blocks * (total > 0 ? w[k] / total : 1.0 / run.size()));
-    tblocks[k] = std::max(1, std::min(want[k], share));
+  for (size_t k = 0; k < T; ++k) {
+    if (!full[k]) {
+      const double share = wfree > 0.0 ? free_blocks * (w[k] / wfree)
+                                       : (double)free_blocks / (double)std::max<size_t>(nfree, 1);
+      tblocks[k] = std::max(1, (int)share);
+      frac.push_back({share - std::floor(share), (int)k});
+    }
     used += tblocks[k];
   }
-  while (used > max_blocks) {                 // rounding left too many: trim the largest
+  std::sort(frac.begin(), frac.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b2) {
+    return a.first != b2.first ? a.first > b2.first : a.second < b2.second;
+  });
+  for (const auto& f : frac) {
+    if (used >= max_blocks) break;
+    if (tblocks[f.second] < want[f.second]) { ++tblocks[f.second]; ++used; }
+  }
+  while (used > max_blocks) {                 // the one-block minimum left too many: trim the largest
     const size_t k = (size_t)(std::max_element(tblocks.begin(), tblocks.end()) - tblocks.begin());
     if (tblocks[k] <= 1) break;
     --tblocks[k];
@@ -727,7 +783,8 @@ static int rebuild(pdlp_batch* b) {
   std::vector<int> rwr, cwr, teams;
   if (tblocks.empty()) {
     const int want = (std::max(b->n_rtiles, b->n_ctiles) + kWarps - 1) / kWarps;
-    const int G = std::max(1, std::min(max_blocks, want));
+    int G = std::max(1, std::min(max_blocks, want));
+    if (b->force_blocks > 0) G = std::min(G, b->force_blocks);
     b->grid = G;
     block_ranges(rw, G * kWarps, rwr);
     block_ranges(cw, G * kWarps, cwr);
@@ -851,6 +908,48 @@ static int infeasibility_test(pdlp_batch* b, Slot& sl, int* request) {
   if (sl.hits >= 2) *request = kind;
   return PDLP_OK;
 }
+
+// ---- tuning cache ---------------------------------------------------------------
+//
+// Tuned choices by nnz profile (pdlp_tune_lp, pdlp_tune_cache_*), shared by
+// every batch of the process; batches with cfg.autotune read it at admission.
+
+namespace {
+
+struct TuneKeyLess {
+  bool operator()(const pdlp_tune_key& a, const pdlp_tune_key& b) const {
+    if (a.rows_bucket != b.rows_bucket) return a.rows_bucket < b.rows_bucket;
+    if (a.row_len_bucket != b.row_len_bucket) return a.row_len_bucket < b.row_len_bucket;
+    return a.col_len_bucket < b.col_len_bucket;
+  }
+};
+
+std::mutex g_tune_mu;
+std::map<pdlp_tune_key, pdlp_tuning, TuneKeyLess> g_tune;
+
+pdlp_tune_key tune_key(int m, int n, long long nnz) {
+  pdlp_tune_key k;
+  k.rows_bucket = (int)std::floor(std::log2((double)m + 1.0));
+  k.row_len_bucket = m > 0 ? (int)std::floor(2.0 * std::log2((double)nnz / m + 1.0)) : 0;
+  k.col_len_bucket = n > 0 ? (int)std::floor(2.0 * std::log2((double)nnz / n + 1.0)) : 0;
+  return k;
+}
+
+bool tuning_valid(const pdlp_tuning& t) {
+  auto pow2 = [](int v) { return v >= 1 && v <= 32 && (v & (v - 1)) == 0; };
+  return pow2(t.lanes_rows) && pow2(t.lanes_cols) && t.tile_rows >= 1 &&
+         t.tile_rows <= kWTileRows && t.tile_nnz >= 1 && t.tile_nnz <= kWTileNnz;
+}
+
+bool tune_lookup(int m, int n, long long nnz, pdlp_tuning* out) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  auto it = g_tune.find(tune_key(m, n, nnz));
+  if (it == g_tune.end()) return false;
+  *out = it->second;
+  return true;
+}
+
+}  // namespace
 
 // ---- admission ---------------------------------------------------------------
 //
@@ -1050,8 +1149,17 @@ static int admit_complete(pdlp_batch* b, Pending& pd, int herr) {
   Inst& I = S.inst;
   std::memset(&I, 0, sizeof(I));
   I.m = m; I.n = n; I.nnz = nnz;
-  I.lanes_r = b->cfg.lanes_override ? b->cfg.lanes_override : lanes_for(nnz, m);
-  I.lanes_c = b->cfg.lanes_override ? b->cfg.lanes_override : lanes_for(nnz, n);
+  // lanes per row and tile shape: forced (tuning runs), tuned (cache), or the
+  // fixed rules
+  pdlp_tuning tn{};
+  const bool tuned = b->force_set ? (tn = b->force, true)
+                                  : (b->cfg.autotune != 0 && tune_lookup(m, n, nnz, &tn));
+  const int tile_rows = tuned ? tn.tile_rows : b->cfg.tile_rows;
+  const int tile_nnz = tuned ? tn.tile_nnz : b->cfg.tile_nnz;
+  I.lanes_r = b->cfg.lanes_override ? b->cfg.lanes_override
+                                    : (tuned ? tn.lanes_rows : lanes_for(nnz, m));
+  I.lanes_c = b->cfg.lanes_override ? b->cfg.lanes_override
+                                    : (tuned ? tn.lanes_cols : lanes_for(nnz, n));
   I.sense = P->sense;
   I.ruiz_iters = prm.scaling == PDLP_SCALING_PDLP ? 10 : (prm.scaling == PDLP_SCALING_RUIZ ? 20 : 0);
   I.use_pc = prm.scaling == PDLP_SCALING_PDLP || prm.scaling == PDLP_SCALING_POCK_CHAMBOLLE;
@@ -1073,6 +1181,7 @@ static int admit_complete(pdlp_batch* b, Pending& pd, int herr) {
   S.xprev = (double*)at(L.nvec[15]);
   S.yprev = (double*)at(L.mvec[14]);
   S.detect = prm.detect_infeasibility != 0;
+  S.expected_iters = std::isfinite(prm.expected_iterations) ? std::max(0.0, prm.expected_iterations) : 0.0;
   S.eps_inf = prm.eps_infeasible > 0.0 ? prm.eps_infeasible : 1e-8;
   I.v0 = has_v0 ? (const double*)at(L.v0) : nullptr;
   I.f32 = f32 ? 1 : 0;
@@ -1089,8 +1198,8 @@ static int admit_complete(pdlp_batch* b, Pending& pd, int herr) {
   I.check_every = prm.check_every; I.stepsize_every = prm.stepsize_every;
   I.beta_s = prm.beta_sufficient; I.beta_n = prm.beta_necessary; I.beta_a = prm.beta_artificial;
   I.theta = prm.primal_weight_smoothing;
-  plan_tiles(pd.rp, m, slot, b->cfg.tile_rows, b->cfg.tile_nnz, S.rt, S.rtw);
-  plan_tiles(pd.cp, n, slot, b->cfg.tile_rows, b->cfg.tile_nnz, S.ct, S.ctw);
+  plan_tiles(pd.rp, m, slot, tile_rows, tile_nnz, S.rt, S.rtw);
+  plan_tiles(pd.cp, n, slot, tile_rows, tile_nnz, S.ct, S.ctw);
   // algorithmic bytes of one PDHG iteration: value + index per
   // entry and pointer per row on both passes, one gathered word per column /
   // row, the vectors each pass reads and writes
@@ -1233,6 +1342,7 @@ void pdlp_params_default(pdlp_params* p) {
   p->history_capacity = 0;
   p->detect_infeasibility = 0;
   p->eps_infeasible = 1e-8;
+  p->expected_iterations = 0.0;
 }
 
 void pdlp_batch_config_default(pdlp_batch_config* c) {
@@ -1245,6 +1355,7 @@ void pdlp_batch_config_default(pdlp_batch_config* c) {
   c->lanes_override = 0;
   c->memory_budget = 0;
   c->barrier_timeout_us = 0;
+  c->autotune = 0;
   c->test_withhold_arrival = 0;
 }
 
@@ -1672,6 +1783,129 @@ int pdlp_batch_cancel(pdlp_batch* b, int32_t slot) {
   int one = 1;
   PDLP_CUDA(cudaMemcpyAsync(&b->d_state[slot].cancel, &one, sizeof(int), cudaMemcpyHostToDevice, b->stream));
   PDLP_CUDA(cudaStreamSynchronize(b->stream));
+  return PDLP_OK;
+}
+
+void pdlp_tune_key_of(int32_t m, int32_t n, int64_t nnz, pdlp_tune_key* key) {
+  if (key) *key = tune_key(m, n, nnz);
+}
+
+int pdlp_tune_cache_size(void) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  return (int)g_tune.size();
+}
+
+int pdlp_tune_cache_get(int32_t i, pdlp_tune_key* key, pdlp_tuning* tuning) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  if (i < 0 || i >= (int)g_tune.size()) return fail(PDLP_ERR_ARG, "no such cache entry");
+  auto it = g_tune.begin();
+  std::advance(it, i);
+  if (key) *key = it->first;
+  if (tuning) *tuning = it->second;
+  return PDLP_OK;
+}
+
+int pdlp_tune_cache_put(const pdlp_tune_key* key, const pdlp_tuning* tuning) {
+  if (!key || !tuning) return fail(PDLP_ERR_ARG, "NULL key or tuning");
+  if (!tuning_valid(*tuning))
+    return fail(PDLP_ERR_ARG, "tuning out of range (lanes 1..32, a power of two; tile_rows 1..64; "
+                              "tile_nnz 1..512)");
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tune[*key] = *tuning;
+  return PDLP_OK;
+}
+
+void pdlp_tune_cache_clear(void) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tune.clear();
+}
+
+int pdlp_tune_lp(const pdlp_problem_desc* prob, const pdlp_params* params, void* stream,
+                 pdlp_tuning* out) {
+  if (!prob) return fail(PDLP_ERR_ARG, "NULL problem");
+  // the probe runs never converge: zero tolerances, no limits
+  pdlp_params prm;
+  pdlp_params_default(&prm);
+  if (params) prm = *params;
+  prm.eps_abs = 0.0; prm.eps_rel = 0.0; prm.feas_cap = 0.0;
+  prm.max_iter = (int64_t)1 << 40;
+  prm.time_limit = 1e9;
+  prm.history_capacity = 0;
+  prm.detect_infeasibility = 0;
+  pdlp_batch_config cfg;
+  pdlp_batch_config_default(&cfg);
+  cfg.max_slots = 1;
+  pdlp_batch* b = nullptr;
+  int rc = pdlp_batch_create(&cfg, stream, &b);
+  if (rc) return rc;
+  constexpr int kSetupSteps = 48;     // scaling (<= 12 steps), set-up, 20 power rounds
+  constexpr int kTimedSteps = 64;
+  // Every candidate runs on the same number of blocks: about eight tiles of
+  // the default shape per warp, the load a warp carries when a full batch
+  // shares the GPU.  Timed alone on all the blocks it can use, an LP favours
+  // small tiles (more warps on one LP), which lose in a loaded batch.
+  {
+    const long long by_nnz = (long long)prob->nnz / default_tile_nnz() + 1;
+    const long long by_rows = (long long)std::max(prob->m, prob->n) / default_tile_rows() + 1;
+    const long long tiles = std::max(by_nnz, by_rows);
+    b->force_blocks = (int)std::max(1LL, (tiles + 8 * kWarps - 1) / (8 * kWarps));
+  }
+  auto probe = [&](const pdlp_tuning& cand, double* us) -> int {
+    b->force_set = true;
+    b->force = cand;
+    int32_t slot = -1, active = 0;
+    int r = pdlp_batch_admit(b, prob, &prm, &slot);
+    if (r) return r;
+    if ((r = pdlp_batch_step(b, kSetupSteps, &active))) return r;
+    double best = INFINITY;
+    for (int rep = 0; rep < 2 && active > 0; ++rep) {
+      if ((r = pdlp_batch_step(b, kTimedSteps, &active))) return r;
+      double ms = 0.0, by = 0.0;
+      int64_t its = 0;
+      pdlp_batch_last_timing(b, &ms, &by, &its);
+      if (its > 0) best = std::min(best, 1000.0 * ms / (double)its);
+    }
+    *us = best;
+    return pdlp_batch_retire(b, slot);
+  };
+  pdlp_tuning def{};
+  def.lanes_rows = lanes_for(prob->nnz, prob->m);
+  def.lanes_cols = lanes_for(prob->nnz, prob->n);
+  def.tile_rows = default_tile_rows();
+  def.tile_nnz = default_tile_nnz();
+  pdlp_tuning best = def;
+  double best_us = INFINITY, def_us = INFINITY;
+  const int lanes[3] = {1, 2, 4};
+  for (int a = 0; a < 3 && !rc; ++a) {
+    for (int c = 0; c < 3 && !rc; ++c) {
+      pdlp_tuning cand = def;
+      cand.lanes_rows = lanes[a];
+      cand.lanes_cols = lanes[c];
+      double us = INFINITY;
+      rc = probe(cand, &us);
+      if (cand.lanes_rows == def.lanes_rows && cand.lanes_cols == def.lanes_cols) def_us = us;
+      if (!rc && us < best_us) { best_us = us; best = cand; }
+    }
+  }
+  const int shapes[3][2] = {{32, 512}, {64, 256}, {32, 256}};
+  for (int k = 0; k < 3 && !rc; ++k) {
+    pdlp_tuning cand = best;
+    cand.tile_rows = shapes[k][0];
+    cand.tile_nnz = shapes[k][1];
+    double us = INFINITY;
+    rc = probe(cand, &us);
+    if (!rc && us < best_us) { best_us = us; best = cand; }
+  }
+  pdlp_batch_destroy(b);
+  if (rc) return rc;
+  if (!std::isfinite(best_us)) return fail(PDLP_ERR_STATE, "tuning: the LP finished inside its probe runs");
+  best.us_per_iteration = best_us;
+  best.default_us_per_iteration = def_us;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune[tune_key(prob->m, prob->n, prob->nnz)] = best;
+  }
+  if (out) *out = best;
   return PDLP_OK;
 }
 

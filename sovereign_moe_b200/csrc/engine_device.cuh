@@ -116,9 +116,15 @@ __device__ __forceinline__ void bulk_stage(void* dst, const void* base, int firs
       ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
 }
 
-// Per-warp phase bits of the two barriers, kept in registers for the launch.
+// Per-warp state kept in registers for the launch: the phase bits of the two
+// copy barriers, and the tiles of the current reduction group whose
+// completion the warp has not counted yet.  A warp counts the tiles of one
+// group that it processes back to back with one atomic, when it leaves the
+// group (`flush`: its next tile lies in another group, or it has none).
 struct BulkPhase {
   unsigned m = 0, v = 0;
+  unsigned pend = 0;
+  bool flush = true;
 };
 
 // ---- reductions -----------------------------------------------------------

@@ -59,17 +59,26 @@ __device__ __forceinline__ double merit(double omega, double p, double d, double
 // instance) sums the group's tile partials in tile order; the warp that
 // completes the instance's last group sums the group partials in group order
 // and advances the state machine.  Returns true in that warp, with the
-// instance's reduced values in res (every lane).
+// instance's reduced values in res (every lane).  A warp that goes on with
+// another tile of the same group only counts this one (ph.pend) and returns
+// false; its atomic, when it leaves the group, counts them all and releases
+// their partials together (every partial is written by lane 0, the lane that
+// issues the atomic).  Which warp completes a group changes nothing in the
+// sums, whose order is the tile order.
 __device__ __forceinline__ bool warp_finish(const EngineArgs& A, const Tile& t, int side,
                                             int g_first, int g_last, bool need_red, Ops ops,
-                                            double* res, int lane) {
+                                            double* res, int lane, BulkPhase& ph) {
+  ph.pend += 1;
+  if (!ph.flush) return false;
+  const unsigned done = ph.pend;
+  ph.pend = 0;
   const int g = t.group;
   const int2 gt = A.group_tiles[g];
   const double* tp = A.partials + (side ? (size_t)A.n_rtiles * kNP : 0);
   unsigned last = 0;
   __syncwarp();
-  if (lane == 0)   // release this tile's partials; acquire the group's if last
-    last = atom_add_acq_rel(A.gcounters + g, 1u) == (unsigned)(gt.y - gt.x - 1);
+  if (lane == 0)   // release these tiles' partials; acquire the group's if last
+    last = atom_add_acq_rel(A.gcounters + g, done) + done == (unsigned)(gt.y - gt.x);
   last = __shfl_sync(kFull, last, 0);
   if (!last) return false;
   __syncwarp();                            // order the lanes' reads after lane 0's acquire
@@ -411,7 +420,7 @@ __device__ void hot_rtile(const EngineArgs& A, const Tile& t, int ti, const Inst
   }
   if (!need_fin) return;
   double res[kNP];
-  if (warp_finish(A, t, 0, I.rg_begin, I.rg_end, need_red, ops, res, lane)) {
+  if (warp_finish(A, t, 0, I.rg_begin, I.rg_end, need_red, ops, res, lane, ph)) {
     if (lane == 0) r_finish(A, I, S, rmode, res);
     __syncwarp();
   }
@@ -489,7 +498,7 @@ __device__ void hot_ctile(const EngineArgs& A, const Tile& t, int ti, const Inst
     }
   }
   double res[kNP];
-  if (warp_finish(A, t, 1, I.cg_begin, I.cg_end, need_red, ops, res, lane)) {
+  if (warp_finish(A, t, 1, I.cg_begin, I.cg_end, need_red, ops, res, lane, ph)) {
     if (lane == 0) c_finish(A, I, S, cmode, res);
     __syncwarp();
   }
@@ -791,7 +800,7 @@ __device__ void process_rtile(const EngineArgs& A, const Tile t, int ti, WarpSme
   }
   if (!need_fin) return;
   double res[kNP];
-  if (warp_finish(A, t, 0, I.rg_begin, I.rg_end, need_red, ops, res, lane)) {
+  if (warp_finish(A, t, 0, I.rg_begin, I.rg_end, need_red, ops, res, lane, ph)) {
     if (lane == 0) r_finish(A, I, S, rmode, res);
     __syncwarp();
   }
@@ -1288,7 +1297,7 @@ __device__ void process_ctile(const EngineArgs& A, const Tile t, int ti, WarpSme
     }
   }
   double res[kNP];
-  if (warp_finish(A, t, 1, I.cg_begin, I.cg_end, need_red, ops, res, lane)) {
+  if (warp_finish(A, t, 1, I.cg_begin, I.cg_end, need_red, ops, res, lane, ph)) {
     if (lane == 0) c_finish(A, I, S, cmode, res);
     __syncwarp();
   }

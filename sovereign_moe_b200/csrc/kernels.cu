@@ -52,19 +52,25 @@ constexpr int kStageUnroll = 8;        // independent loads per lane in flight
 
 // Variants of the row-block pass (pdlp_spmv_*_ex): streamed where a run of
 // rows fits the staging buffer, or the row-group path for every block.
-enum SpmvVariant : int { SPMV_AUTO = 0, SPMV_STREAMED = 1, SPMV_ROW_GROUPS = 2 };
+enum SpmvVariant : int { SPMV_AUTO = 0, SPMV_STREAMED = 1, SPMV_ROW_GROUPS = 2, SPMV_BANDED = 3 };
+constexpr int kBandCap = 3072;         // x entries a block stages (banded variant)
 
 // Streams the rows i0 .. i1-1 of the warp's block (rows r0 + i), whose
 // entries are [p0, p0 + cnt), cnt <= kStageEntries: coalesced, independent
 // loads of indices and values, every gather at once, products staged in
 // shared memory; lane i then sums row i in storage order.
+//
+// With a band (banded variant), x[blo, blo + bcnt) is already in shared memory
+// and the gathers that fall in it read from there.
 template <typename T>
 __device__ __forceinline__ void spmv_rows_staged(int r0, int i0, int i1, long long rs,
                                                  long long re, long long p0, int cnt, int lane,
                                                  const int* __restrict__ ri,
                                                  const T* __restrict__ rx,
                                                  const T* __restrict__ x, T* __restrict__ y,
-                                                 T* __restrict__ prod) {
+                                                 T* __restrict__ prod,
+                                                 const T* band = nullptr, int blo = 0,
+                                                 int bcnt = 0) {
   for (int q0 = 0; q0 < cnt; q0 += kStageUnroll * 32) {
     int idx[kStageUnroll];
     T val[kStageUnroll];
@@ -78,7 +84,8 @@ __device__ __forceinline__ void spmv_rows_staged(int r0, int i0, int i1, long lo
 #pragma unroll
     for (int u = 0; u < kStageUnroll; ++u) {
       const int q = q0 + u * 32 + lane;
-      xv[u] = q < cnt ? __ldg(x + idx[u]) : T(0);
+      const unsigned off = (unsigned)(idx[u] - blo);
+      xv[u] = q < cnt ? (off < (unsigned)bcnt ? band[off] : __ldg(x + idx[u])) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < kStageUnroll; ++u) {
@@ -188,6 +195,98 @@ __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_rows32_kernel(
   }
 }
 
+// Banded variant: one block per 256 consecutive rows (a warp per 32), no
+// grid stride.  The block first reads the indices of its streamable runs
+// (the same runs the streamed variant forms) and reduces their smallest and
+// largest; when that span fits kBandCap entries (3072), the block loads x over it
+// into shared memory with coalesced loads, and the runs' gathers read from
+// there instead of from L2.  This pays on banded matrices (a multi-period
+// plan: a block of rows touches the columns of one or two periods), where
+// the gathers of the streamed variant are bound by L2 sector traffic.  Rows
+// outside the runs take the row-group path with global gathers, long rows
+// the second launch, as in the other variants.
+template <typename T>
+__global__ void __launch_bounds__(kSpmvWarps * 32) spmv_band_kernel(
+    int m, const int64_t* __restrict__ rp, const int* __restrict__ ri,
+    const T* __restrict__ rx, const T* __restrict__ x, T* __restrict__ y,
+    int* __restrict__ long_rows) {
+  __shared__ T stage[kSpmvWarps][kStageEntries];
+  __shared__ T band[kBandCap];
+  __shared__ int wlo[kSpmvWarps], whi[kSpmvWarps];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const long long nblk = ((long long)m + 31) / 32;
+  const long long b = (long long)blockIdx.x * kSpmvWarps + w;
+  const bool have = b < nblk;                       // warp-uniform
+  const int r0 = have ? (int)(b * 32) : 0;
+  const int nr = have ? min(32, m - r0) : 0;
+  const long long rs = lane < nr ? (long long)__ldg(rp + r0 + lane) : 0LL;
+  const long long re = lane < nr ? (long long)__ldg(rp + r0 + lane + 1) : 0LL;
+  const bool is_long = lane < nr && re - rs > kLongRow;
+  if (is_long) {
+    const int slot = atomicAdd(long_rows, 1);
+    if (slot < m) long_rows[2 + slot] = r0 + lane;
+  }
+  const unsigned long_mask = __ballot_sync(kAll, is_long);
+  const unsigned rows_mask = nr == 32 ? kAll : (nr > 0 ? ((1u << nr) - 1u) : 0u);
+  // the runs: the whole block, else each half of 16 rows that fits
+  int ra[2] = {0, 0}, rb[2] = {0, 0}, nrun = 0;
+  long long qa[2] = {0, 0}, qn[2] = {0, 0};
+  if (have) {
+    const long long pa = __shfl_sync(kAll, rs, 0), pb = __shfl_sync(kAll, re, nr - 1);
+    if (long_mask == 0u && pb - pa <= kStageEntries) {
+      ra[0] = 0; rb[0] = nr; qa[0] = pa; qn[0] = pb - pa; nrun = 1;
+    } else {
+      for (int h = 0; h < 2 && 16 * h < nr; ++h) {
+        const int i0 = 16 * h, i1 = min(nr, i0 + 16);
+        const unsigned hb = (i1 - i0 == 16 ? 0xffffu : ((1u << (i1 - i0)) - 1u)) << i0;
+        const long long ha = __shfl_sync(kAll, rs, i0), hz = __shfl_sync(kAll, re, i1 - 1);
+        if ((long_mask & hb) == 0u && hz - ha <= kStageEntries) {
+          ra[nrun] = i0; rb[nrun] = i1; qa[nrun] = ha; qn[nrun] = hz - ha; ++nrun;
+        }
+      }
+    }
+  }
+  // the span of the runs' indices, over the block
+  int lo = 0x7fffffff, hi = -1;
+  for (int k = 0; k < nrun; ++k)
+    for (int q = lane; q < (int)qn[k]; q += 32) {
+      const int j = __ldg(ri + qa[k] + q);
+      lo = min(lo, j);
+      hi = max(hi, j);
+    }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    lo = min(lo, __shfl_xor_sync(kAll, lo, off));
+    hi = max(hi, __shfl_xor_sync(kAll, hi, off));
+  }
+  if (lane == 0) { wlo[w] = lo; whi[w] = hi; }
+  __syncthreads();
+  int blo = 0x7fffffff, bhi = -1;
+  for (int k = 0; k < kSpmvWarps; ++k) { blo = min(blo, wlo[k]); bhi = max(bhi, whi[k]); }
+  const int bcnt = (bhi >= blo && bhi - blo < kBandCap) ? bhi - blo + 1 : 0;   // block-uniform
+  for (int i = threadIdx.x; i < bcnt; i += kSpmvWarps * 32) band[i] = __ldg(x + blo + i);
+  __syncthreads();
+  unsigned skip = long_mask;
+  for (int k = 0; k < nrun; ++k) {
+    spmv_rows_staged<T>(r0, ra[k], rb[k], rs, re, qa[k], (int)qn[k], lane, ri, rx, x, y, stage[w],
+                        band, blo, bcnt);
+    skip |= (rb[k] - ra[k] == 32 ? kAll : ((1u << (rb[k] - ra[k])) - 1u) << ra[k]);
+  }
+  if (!have || (skip & rows_mask) == rows_mask) return;
+  const bool mine = lane < nr && !((skip >> lane) & 1u);
+  long long len = mine ? re - rs : 0;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) len += __shfl_xor_sync(kAll, len, off);
+  const int left = __popc(rows_mask & ~skip);
+  const long long avg = left > 0 ? (len + left - 1) / left : 0;
+  if (avg <= 1) spmv_block_rows<T, 1>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
+  else if (avg <= 2) spmv_block_rows<T, 2>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
+  else if (avg <= 4) spmv_block_rows<T, 4>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
+  else if (avg <= 8) spmv_block_rows<T, 8>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
+  else if (avg <= 16) spmv_block_rows<T, 16>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
+  else spmv_block_rows<T, 32>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_long_rows_kernel(
     const int64_t* __restrict__ rp, const int* __restrict__ ri, const T* __restrict__ rx,
@@ -273,7 +372,7 @@ template <typename T>
 int launch_spmv(int m, const int64_t* rp, const int* ri, const T* rx, const T* x, T* y,
                 cudaStream_t st, int variant = SPMV_AUTO) {
   if (m < 0) return fail(PDLP_ERR_ARG, "m must be >= 0");
-  if (variant < SPMV_AUTO || variant > SPMV_ROW_GROUPS) return fail(PDLP_ERR_ARG, "unknown SpMV variant");
+  if (variant < SPMV_AUTO || variant > SPMV_BANDED) return fail(PDLP_ERR_ARG, "unknown SpMV variant");
   if (m == 0) return PDLP_OK;
   if (!rp || !ri || !rx || !x || !y) return fail(PDLP_ERR_ARG, "NULL pointer");
   int* long_rows = nullptr;
@@ -281,7 +380,13 @@ int launch_spmv(int m, const int64_t* rp, const int* ri, const T* rx, const T* x
   if (rc != PDLP_OK) return rc;
   const long long nblk = ((long long)m + 31) / 32;
   const int g = (int)std::min((nblk + kSpmvWarps - 1) / kSpmvWarps, 1LL << 30);
-  spmv_rows32_kernel<T><<<g, kSpmvWarps * 32, 0, st>>>(m, rp, ri, rx, x, y, long_rows, variant);
+  if (variant == SPMV_BANDED) {
+    const long long gb = (nblk + kSpmvWarps - 1) / kSpmvWarps;
+    if (gb > (1LL << 31) - 1) return fail(PDLP_ERR_ARG, "m too large for the banded variant");
+    spmv_band_kernel<T><<<(int)gb, kSpmvWarps * 32, 0, st>>>(m, rp, ri, rx, x, y, long_rows);
+  } else {
+    spmv_rows32_kernel<T><<<g, kSpmvWarps * 32, 0, st>>>(m, rp, ri, rx, x, y, long_rows, variant);
+  }
   spmv_long_rows_kernel<T><<<592, kSpmvWarps * 32, 0, st>>>(rp, ri, rx, x, y, m, long_rows);
   count_launches(2);
   PDLP_CUDA(cudaGetLastError());
@@ -301,11 +406,11 @@ int tune_spmv(int m, const int64_t* rp, const int* ri, const T* rx, const T* x, 
   PDLP_CUDA(cudaEventCreate(&e0));
   const cudaError_t ce = cudaEventCreate(&e1);
   if (ce != cudaSuccess) { cudaEventDestroy(e0); return cuda_fail(ce, "cudaEventCreate"); }
-  const int variants[2] = {SPMV_STREAMED, SPMV_ROW_GROUPS};
+  const int variants[3] = {SPMV_STREAMED, SPMV_ROW_GROUPS, SPMV_BANDED};
   double best_ms = 0.0;
   int rc = PDLP_OK;
   *best = SPMV_STREAMED;
-  for (int k = 0; k < 2 && rc == PDLP_OK; ++k) {
+  for (int k = 0; k < 3 && rc == PDLP_OK; ++k) {
     rc = launch_spmv<T>(m, rp, ri, rx, x, y, st, variants[k]);
     if (rc != PDLP_OK) break;
     cudaEventRecord(e0, st);

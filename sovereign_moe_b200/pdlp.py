@@ -57,6 +57,10 @@ class PDLPParams:
     # iteration or time limit; off by default, as the reference has no such test
     detect_infeasibility: bool = False
     eps_infeasible: float = 1e-8
+    # B200 engine only: the iterations this LP is expected to need (0 = no
+    # estimate), a hint for sizing block teams in a batch; results do not
+    # depend on it
+    expected_iterations: float = 0.0
 
 
 @dataclass
@@ -133,6 +137,7 @@ def params_struct(params: PDLPParams, n: int, time_used: float = 0.0, history_ca
     p.precision = _lib.PRECISION[prec]
     p.detect_infeasibility = 1 if getattr(params, "detect_infeasibility", False) else 0
     p.eps_infeasible = float(getattr(params, "eps_infeasible", 1e-8))
+    p.expected_iterations = float(getattr(params, "expected_iterations", 0.0))
     p.time_used = float(time_used)
     if history_capacity is None:
         history_capacity = int(min(params.max_iter // max(params.check_every, 1) + 1, 1 << 20))

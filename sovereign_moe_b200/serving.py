@@ -34,6 +34,7 @@ import numpy as np
 from . import _lib
 from .batch import BatchEngine
 from .pdlp import PDLPParams, solve_pdlp
+from .schedule import IterationModel
 
 __all__ = ["Request", "Server", "serve_one_at_a_time", "latency_summary"]
 
@@ -88,6 +89,9 @@ class Server:
         self.chunk_steps = int(chunk_steps)
         self.queue: deque = deque()
         self.inflight: dict = {}
+        # iteration estimates learned from the requests served so far: the
+        # engine gives the LPs expected to run longest their blocks first
+        self.model = IterationModel()
 
     def close(self):
         self.engine.close()
@@ -102,7 +106,8 @@ class Server:
         while self.queue and len(self.inflight) < self.max_slots:
             req = self.queue[0]
             try:
-                slot = self.engine.admit(req.problem, self.params)
+                slot = self.engine.admit(req.problem, self.params,
+                                         hint=self.model.predict(req.problem))
             except _lib.PDLPError as exc:
                 if exc.code == _lib.PDLP_ERR_OOM:
                     stats.refused_for_memory += 1
@@ -123,6 +128,7 @@ class Server:
                 req = self.inflight.pop(slot)
                 req.solution = self.engine.fetch(slot)
                 req.finished = now()
+                self.model.observe(req.problem, req.solution.iterations)
                 self.engine.retire(slot)
                 stats.completed += 1
                 stats.latencies.append(req.latency)

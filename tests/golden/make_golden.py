@@ -138,4 +138,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {os.path.basename(__file__)} REFERENCE_ROOT  "
+                 "(the root of the reference source tree, holding src/sovopt)")
+    main(sys.argv[1])

@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_defaults_match_reference_params():
     lib = _lib.load()
-    assert lib.pdlp_abi_version() == 3
+    assert lib.pdlp_abi_version() == 4
     p = _lib.Params()
     lib.pdlp_params_default(ctypes.byref(p))
     ref = PDLPParams()
@@ -46,19 +46,23 @@ def test_abi_version_and_defaults_match_reference_params():
     # the fields after the reference's: written by the C default at the same offsets
     assert p.precision == _lib.PRECISION["fp64"]
     assert p.detect_infeasibility == 0 and p.eps_infeasible == 1e-8
+    assert p.expected_iterations == 0.0    # no scheduling hint
     assert ref.detect_infeasibility is False and ref.eps_infeasible == 1e-8
 
 
 def test_struct_layouts_match_the_header():
     # sizes of the C structs on x86-64 (natural alignment)
     assert ctypes.sizeof(_lib.ProblemDesc) == 4 + 4 + 8 + 12 * 8 + 8 + 4 + 4
-    # six int32, memory_budget, barrier_timeout_us, test_withhold_arrival (+pad)
-    assert ctypes.sizeof(_lib.BatchConfig) == 6 * 4 + 8 + 8 + 8
+    # six int32, memory_budget, barrier_timeout_us, autotune, test_withhold_arrival
+    assert ctypes.sizeof(_lib.BatchConfig) == 6 * 4 + 8 + 8 + 4 + 4
+    assert ctypes.sizeof(_lib.TuneKey) == 12
+    assert ctypes.sizeof(_lib.Tuning) == 4 * 4 + 2 * 8
     # ..., history_len (+pad), device_seconds, device_start_ns, device_end_ns
     assert ctypes.sizeof(_lib.Result) == 8 + 3 * 8 + 9 * 8 + 8 + 8 + 2 * 8
     # eps..time_limit, check/stepsize, betas + smoothing, scaling (+pad), power_start,
-    # time_used, history_capacity + precision, detect (+pad), eps_infeasible
-    assert ctypes.sizeof(_lib.Params) == 5 * 8 + 8 + 4 * 8 + 8 + 8 + 8 + 8 + 8 + 8
+    # time_used, history_capacity + precision, detect (+pad), eps_infeasible,
+    # expected_iterations
+    assert ctypes.sizeof(_lib.Params) == 5 * 8 + 8 + 4 * 8 + 8 + 8 + 8 + 8 + 8 + 8 + 8
 
 
 def test_batch_config_defaults():
@@ -68,6 +72,7 @@ def test_batch_config_defaults():
     assert c.block_threads == 128          # the only block size the engine accepts
     assert c.persistent == 1 and c.max_slots == 1
     assert c.barrier_timeout_us == 0       # 0 = the 4 s default
+    assert c.autotune == 0                 # the fixed rules unless asked
     assert c.test_withhold_arrival == 0    # the timeout test hook is off
 
 
@@ -103,3 +108,30 @@ def test_bnr_engine_refuses_the_cpu_and_fails_loudly_without_a_gpu():
     if not torch.cuda.is_available():
         with pytest.raises(RuntimeError, match="GPU backend unavailable"):
             BNREngine(prob, SimpleNamespace(obj=1.0), BNRConfig(batch=2, device="gpu"))
+
+
+def test_tuning_cache_api_without_a_gpu(tmp_path):
+    """The tuner's cache: profile keys, checked entries, save and load."""
+    from sovereign_moe_b200 import tuning
+    tuning.clear()
+    assert tuning.entries() == []
+    k = tuning.profile_key(1000, 4000, 32000)
+    # log2(1001) = 9.97; 2 log2(33) = 10.09; 2 log2(9) = 6.34
+    assert k == (9, 10, 6)
+    assert tuning.profile_key(0, 5, 0) == (0, 0, 0)
+    lib = _lib.load()
+    key = _lib.TuneKey(*k)
+    good = _lib.Tuning(2, 1, 32, 256, 11.5, 12.0)
+    assert lib.pdlp_tune_cache_put(ctypes.byref(key), ctypes.byref(good)) == _lib.PDLP_OK
+    for bad in (_lib.Tuning(3, 1, 32, 256, 1, 1), _lib.Tuning(1, 1, 65, 256, 1, 1),
+                _lib.Tuning(1, 1, 32, 513, 1, 1), _lib.Tuning(0, 1, 32, 256, 1, 1)):
+        assert lib.pdlp_tune_cache_put(ctypes.byref(key), ctypes.byref(bad)) == _lib.PDLP_ERR_ARG
+    e = tuning.entries()
+    assert len(e) == 1 and e[0]["key"] == list(k) and e[0]["lanes_rows"] == 2
+    path = tmp_path / "tune.json"
+    tuning.save(path)
+    tuning.clear()
+    assert tuning.entries() == []
+    assert tuning.load(path) == 1
+    assert tuning.entries() == e
+    tuning.clear()

@@ -179,3 +179,17 @@ def test_admit_many_refuses_only_the_bad_lp(require_gpu):
         got = [eng.fetch(s) for s in slots if s >= 0]
     for p, t in zip([good[0], good[1], good[2], good[3]], got):
         _same(t, _alone(p))
+
+
+def test_scheduling_hints_change_no_result(require_gpu):
+    """Expected-iteration hints resize the block teams (the LPs expected to
+    run longest get their blocks first) but every LP's result stays bitwise
+    the one without hints."""
+    probs = [k.problem for k in uneven_batch(seed=9, count=12, m_lo=80, m_hi=2500)]
+    with BatchEngine(max_slots=12) as eng:
+        plain = eng.solve_all(probs, P6)
+    hints = [50.0 * (i + 1) ** 2 for i in range(len(probs))]     # deliberately uneven
+    with BatchEngine(max_slots=12) as eng:
+        hinted = eng.solve_all(probs, P6, hints=hints)
+    for a, b in zip(plain, hinted):
+        _same(a, b)

@@ -115,11 +115,12 @@ def _spmv_ex(bk, variant, A, x, poison=12345.0, f32=False):
     return out.cpu().numpy()
 
 
-@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("variant", [1, 2, 3])
 def test_spmv_variants_match_oracle(bk, variant):
-    """Both row-block variants (streamed runs of rows, row groups) on rows of
-    every length class: empty, short, up to the staging buffer, long (the
-    second launch), mixed within one 32-row block and its 16-row halves."""
+    """Every row-block variant (streamed runs of rows, row groups, banded) on
+    rows of every length class: empty, short, up to the staging buffer, long
+    (the second launch), mixed within one 32-row block and its 16-row halves.
+    The 2000 columns fit the banded variant's shared-memory band."""
     rng = np.random.default_rng(40 + variant)
     lens = rng.choice([0, 1, 3, 7, 8, 9, 15, 16, 17, 40, 100, 255, 256, 257, 600], size=203)
     m, n = len(lens), 2000
@@ -132,16 +133,33 @@ def test_spmv_variants_match_oracle(bk, variant):
     np.testing.assert_allclose(_spmv_ex(bk, variant, A, x, f32=True), exp, rtol=1e-4, atol=1e-3)
 
 
-def test_streamed_rows_equal_oracle_bitwise(bk):
+@pytest.mark.parametrize("variant", [1, 3])
+def test_streamed_rows_equal_oracle_bitwise(bk, variant):
     """Rows of at most 16 entries are always streamed (every 16-row half fits
     the 256-entry buffer), and a streamed row is the oracle's storage-order
-    sum of rounded products, bit for bit."""
+    sum of rounded products, bit for bit, whether x is gathered from global
+    memory or from the banded variant's shared-memory copy."""
     A, rng = _random_csr(5000, 3000, 4, seed=9)          # about 2.4 entries per row
     lens = np.diff(A.rp)
     assert lens.max() <= 16
     x = rng.standard_normal(A.n)
-    got = _spmv_ex(bk, 1, A, x)
+    got = _spmv_ex(bk, variant, A, x)
     assert np.array_equal(got, po.spmv(A.rp, A.ri, A.rx, x))
+
+
+def test_banded_variant_on_a_band_wider_than_shared_memory(bk):
+    """Blocks whose index span exceeds the band gather from global memory;
+    a banded matrix whose blocks fit stages them; both agree with the oracle."""
+    from sovereign_moe_b200.workloads import blending_plan
+    wide, rng = _random_csr(20_000, 100_000, 1, seed=13)  # 5 per row; spans far beyond 3072
+    x = rng.standard_normal(wide.n)
+    np.testing.assert_allclose(_spmv_ex(bk, 3, wide, x), po.spmv(wide.rp, wide.ri, wide.rx, x),
+                               rtol=1e-12, atol=1e-12)
+    A = blending_plan(seed=1, m=20_000, n=60_000, periods=72, coupling=10).problem.A
+    x = rng.standard_normal(A.n)
+    exp = po.spmv(A.rp, A.ri, A.rx, x)
+    np.testing.assert_allclose(_spmv_ex(bk, 3, A, x), exp, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(_spmv_ex(bk, 3, A, x, f32=True), exp, rtol=1e-4, atol=1e-2)
 
 
 def test_spmv_tuner_and_autotuned_backend(bk):
@@ -155,14 +173,15 @@ def test_spmv_tuner_and_autotuned_backend(bk):
     rp, ri, rx, xd = bk.pointer(A.rp), bk.index(A.ri), bk.to_device(A.rx), bk.to_device(x)
     out = bk.zeros(A.m) + 12345.0
     best = ctypes.c_int32(-1)
-    ms = (ctypes.c_double * 2)()
+    ms = (ctypes.c_double * 3)()
     _lib.check(bk.lib.pdlp_spmv_tune_f64(A.m, rp.data_ptr(), ri.data_ptr(), rx.data_ptr(),
                                          xd.data_ptr(), out.data_ptr(),
                                          ctypes.c_void_p(torch.cuda.current_stream().cuda_stream),
                                          5, ctypes.byref(best), ms))
-    assert best.value in (_lib.PDLP_SPMV_STREAMED, _lib.PDLP_SPMV_ROW_GROUPS)
-    assert ms[0] > 0 and ms[1] > 0
-    assert ms[best.value - 1] == min(ms[0], ms[1])
+    assert best.value in (_lib.PDLP_SPMV_STREAMED, _lib.PDLP_SPMV_ROW_GROUPS,
+                          _lib.PDLP_SPMV_BANDED)
+    assert min(ms) > 0
+    assert ms[best.value - 1] == min(ms)
     np.testing.assert_allclose(out.cpu().numpy(), exp, rtol=1e-12, atol=1e-12)
     tuned = Backend("gpu", autotune=True)
     for _ in range(2):                                   # tunes, then uses the choice

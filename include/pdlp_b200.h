@@ -319,10 +319,10 @@ int pdlp_spmv_f64(int32_t m, const int64_t* rp, const int32_t* ri, const double*
 int pdlp_spmv_f32(int32_t m, const int64_t* rp, const int32_t* ri, const float* rx,
                   const float* x, float* y, void* stream);
 /* The same with an explicit variant of the row-block pass (the plain calls
- * use PDLP_SPMV_STREAMED).  STREAMED: a run of rows whose entries fit a warp's
- * 256-entry buffer is loaded with independent coalesced loads, its products
- * staged in shared memory and each row summed in storage order; other rows
- * take the row-group path.  ROW_GROUPS: every row takes the row-group path
+ * use PDLP_SPMV_STREAMED).  STREAMED: every row of at most 256 entries is
+ * streamed, in runs of consecutive rows whose entries fit a warp's 256-entry
+ * buffer: independent coalesced loads, products staged in shared memory,
+ * each row summed in storage order.  ROW_GROUPS: every row takes the row-group path
  * (L lanes per row from the block's mean row length, strided sums then a
  * xor butterfly).  BANDED: as STREAMED, but a block of 256 rows whose
  * streamed entries' column indices span at most 3072 columns first loads x

@@ -27,18 +27,19 @@ int grid_1d(long long n, int per = kT) {
 // more than kLongRow entries are not summed here: the warp appends them to a
 // list (order immaterial) and leaves them to the second launch.
 //
-// A block without long rows whose entries fit the warp's staging buffer
-// (kStageEntries; the common case for sparse LPs) is streamed: its entries
-// are one contiguous range of the CSR arrays, so the warp loads indices and
-// values with coalesced, mutually independent loads, gathers every x it needs
-// at once, and stages the products in shared memory.  Each lane then sums one
-// row from the buffer in storage order.  The latency of a block is two memory
-// round trips, however many rows it has.
+// Streamed variant (the default): the warp splits its block's short rows into
+// runs of consecutive rows whose entries fit its staging buffer
+// (kStageEntries).  A run's entries are one contiguous range of the CSR
+// arrays, so the warp loads indices and values with coalesced, mutually
+// independent loads, gathers every x it needs at once, and stages the
+// products in shared memory.  Each lane then sums one row from the buffer in
+// storage order.  A run costs two memory round trips, however many rows it
+// has.
 //
-// Other blocks (long rows, or more entries than the buffer) take the row-
-// group path: the warp picks L lanes per row from the block's mean row length
-// (a power of two, 1..32); each lane sums its strided entries in order, a xor
-// butterfly over the L lanes combines them, and 32/L rows run side by side.
+// Row-group variant: the warp picks L lanes per row from the block's mean
+// row length (a power of two, 1..32); each lane sums its strided entries in
+// order, a xor butterfly over the L lanes combines them, and 32/L rows run
+// side by side.
 //
 // spmv_long_rows_kernel: one block of 8 warps per listed long row (grid-
 // stride).  Chunk c of the row goes to warp c mod 8, which keeps a per-lane
@@ -111,6 +112,22 @@ __device__ __forceinline__ void spmv_rows_staged(int r0, int i0, int i1, long lo
   __syncwarp();
 }
 
+// The run of rows that starts at row `start` of a warp's block (a short row):
+// the consecutive short rows from there whose entries fit the staging buffer
+// together.  Rows are contiguous in storage, so the run's entries are one
+// range; a long row, the buffer's capacity or the block's end closes it.
+// Returns the run's end (exclusive), the same in every lane.
+__device__ __forceinline__ int spmv_next_run(int start, int nr, long long rs, long long re,
+                                             unsigned long_mask, int lane) {
+  const long long base = __shfl_sync(kAll, rs, start);
+  const bool ok = lane >= start && lane < nr && !((long_mask >> lane) & 1u) &&
+                  re - base <= kStageEntries;
+  const unsigned fit = __ballot_sync(kAll, ok) >> start;    // bit 0: row `start`
+  const unsigned gap = ~fit;
+  const int len = gap ? __ffs(gap) - 1 : 32 - start;
+  return start + len;
+}
+
 template <typename T, int L>
 __device__ __forceinline__ void spmv_block_rows(int r0, int nr, long long rs, long long re,
                                                 unsigned long_mask, int lane,
@@ -160,24 +177,17 @@ __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_rows32_kernel(
     const unsigned rows_mask = nr == 32 ? kAll : ((1u << nr) - 1u);
     unsigned skip = long_mask;                  // rows the row-group path leaves alone
     if (variant != SPMV_ROW_GROUPS) {
-      // the whole block, else each half of 16 rows, streamed when it has no
-      // long row and its entries fit the buffer
-      const long long pa = __shfl_sync(kAll, rs, 0), pb = __shfl_sync(kAll, re, nr - 1);
-      if (long_mask == 0u && pb - pa <= kStageEntries) {
-        spmv_rows_staged<T>(r0, 0, nr, rs, re, pa, (int)(pb - pa), lane, ri, rx, x, y, stage[w]);
-        continue;
+      // every short row, in runs that fit the buffer; long rows are left to
+      // the second launch
+      for (int start = 0; start < nr;) {
+        if ((long_mask >> start) & 1u) { ++start; continue; }
+        const int end = spmv_next_run(start, nr, rs, re, long_mask, lane);
+        const long long qa = __shfl_sync(kAll, rs, start), qb = __shfl_sync(kAll, re, end - 1);
+        spmv_rows_staged<T>(r0, start, end, rs, re, qa, (int)(qb - qa), lane, ri, rx, x, y,
+                            stage[w]);
+        start = end;
       }
-      for (int h = 0; h < 2 && 16 * h < nr; ++h) {
-        const int i0 = 16 * h, i1 = min(nr, i0 + 16);
-        const unsigned hb = (i1 - i0 == 16 ? 0xffffu : ((1u << (i1 - i0)) - 1u)) << i0;
-        const long long qa = __shfl_sync(kAll, rs, i0), qb = __shfl_sync(kAll, re, i1 - 1);
-        if ((long_mask & hb) == 0u && qb - qa <= kStageEntries) {
-          spmv_rows_staged<T>(r0, i0, i1, rs, re, qa, (int)(qb - qa), lane, ri, rx, x, y,
-                              stage[w]);
-          skip |= hb;
-        }
-      }
-      if ((skip & rows_mask) == rows_mask) continue;
+      continue;
     }
     // mean length of the rows left -> lanes per row
     const bool mine = lane < nr && !((skip >> lane) & 1u);
@@ -196,15 +206,12 @@ __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_rows32_kernel(
 }
 
 // Banded variant: one block per 256 consecutive rows (a warp per 32), no
-// grid stride.  The block first reads the indices of its streamable runs
-// (the same runs the streamed variant forms) and reduces their smallest and
-// largest; when that span fits kBandCap entries (3072), the block loads x over it
-// into shared memory with coalesced loads, and the runs' gathers read from
-// there instead of from L2.  This pays on banded matrices (a multi-period
-// plan: a block of rows touches the columns of one or two periods), where
-// the gathers of the streamed variant are bound by L2 sector traffic.  Rows
-// outside the runs take the row-group path with global gathers, long rows
-// the second launch, as in the other variants.
+// grid stride.  The block first reads the indices of its short rows (the
+// entries the runs will stage) and reduces their smallest and largest; when
+// that span fits kBandCap entries (3072), the block loads x over it into
+// shared memory with coalesced loads, and the runs' gathers read from there
+// instead of from L2.  Long rows go to the second launch, as in the other
+// variants.
 template <typename T>
 __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_band_kernel(
     int m, const int64_t* __restrict__ rp, const int* __restrict__ ri,
@@ -227,33 +234,20 @@ __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_band_kernel(
     if (slot < m) long_rows[2 + slot] = r0 + lane;
   }
   const unsigned long_mask = __ballot_sync(kAll, is_long);
-  const unsigned rows_mask = nr == 32 ? kAll : (nr > 0 ? ((1u << nr) - 1u) : 0u);
-  // the runs: the whole block, else each half of 16 rows that fits
-  int ra[2] = {0, 0}, rb[2] = {0, 0}, nrun = 0;
-  long long qa[2] = {0, 0}, qn[2] = {0, 0};
-  if (have) {
-    const long long pa = __shfl_sync(kAll, rs, 0), pb = __shfl_sync(kAll, re, nr - 1);
-    if (long_mask == 0u && pb - pa <= kStageEntries) {
-      ra[0] = 0; rb[0] = nr; qa[0] = pa; qn[0] = pb - pa; nrun = 1;
-    } else {
-      for (int h = 0; h < 2 && 16 * h < nr; ++h) {
-        const int i0 = 16 * h, i1 = min(nr, i0 + 16);
-        const unsigned hb = (i1 - i0 == 16 ? 0xffffu : ((1u << (i1 - i0)) - 1u)) << i0;
-        const long long ha = __shfl_sync(kAll, rs, i0), hz = __shfl_sync(kAll, re, i1 - 1);
-        if ((long_mask & hb) == 0u && hz - ha <= kStageEntries) {
-          ra[nrun] = i0; rb[nrun] = i1; qa[nrun] = ha; qn[nrun] = hz - ha; ++nrun;
-        }
-      }
-    }
-  }
-  // the span of the runs' indices, over the block
+  // the span of the short rows' indices (the entries the runs will stage),
+  // over the block
   int lo = 0x7fffffff, hi = -1;
-  for (int k = 0; k < nrun; ++k)
-    for (int q = lane; q < (int)qn[k]; q += 32) {
-      const int j = __ldg(ri + qa[k] + q);
+  for (int start = 0; start < nr;) {
+    if ((long_mask >> start) & 1u) { ++start; continue; }
+    const int end = spmv_next_run(start, nr, rs, re, long_mask, lane);
+    const long long qa = __shfl_sync(kAll, rs, start), qb = __shfl_sync(kAll, re, end - 1);
+    for (long long q = qa + lane; q < qb; q += 32) {
+      const int j = __ldg(ri + q);
       lo = min(lo, j);
       hi = max(hi, j);
     }
+    start = end;
+  }
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
     lo = min(lo, __shfl_xor_sync(kAll, lo, off));
@@ -266,25 +260,14 @@ __global__ void __launch_bounds__(kSpmvWarps * 32) spmv_band_kernel(
   const int bcnt = (bhi >= blo && bhi - blo < kBandCap) ? bhi - blo + 1 : 0;   // block-uniform
   for (int i = threadIdx.x; i < bcnt; i += kSpmvWarps * 32) band[i] = __ldg(x + blo + i);
   __syncthreads();
-  unsigned skip = long_mask;
-  for (int k = 0; k < nrun; ++k) {
-    spmv_rows_staged<T>(r0, ra[k], rb[k], rs, re, qa[k], (int)qn[k], lane, ri, rx, x, y, stage[w],
+  for (int start = 0; start < nr;) {
+    if ((long_mask >> start) & 1u) { ++start; continue; }
+    const int end = spmv_next_run(start, nr, rs, re, long_mask, lane);
+    const long long qa = __shfl_sync(kAll, rs, start), qb = __shfl_sync(kAll, re, end - 1);
+    spmv_rows_staged<T>(r0, start, end, rs, re, qa, (int)(qb - qa), lane, ri, rx, x, y, stage[w],
                         band, blo, bcnt);
-    skip |= (rb[k] - ra[k] == 32 ? kAll : ((1u << (rb[k] - ra[k])) - 1u) << ra[k]);
+    start = end;
   }
-  if (!have || (skip & rows_mask) == rows_mask) return;
-  const bool mine = lane < nr && !((skip >> lane) & 1u);
-  long long len = mine ? re - rs : 0;
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) len += __shfl_xor_sync(kAll, len, off);
-  const int left = __popc(rows_mask & ~skip);
-  const long long avg = left > 0 ? (len + left - 1) / left : 0;
-  if (avg <= 1) spmv_block_rows<T, 1>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
-  else if (avg <= 2) spmv_block_rows<T, 2>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
-  else if (avg <= 4) spmv_block_rows<T, 4>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
-  else if (avg <= 8) spmv_block_rows<T, 8>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
-  else if (avg <= 16) spmv_block_rows<T, 16>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
-  else spmv_block_rows<T, 32>(r0, nr, rs, re, skip, lane, ri, rx, x, y);
 }
 
 template <typename T>

@@ -119,7 +119,7 @@ def _spmv_ex(bk, variant, A, x, poison=12345.0, f32=False):
 def test_spmv_variants_match_oracle(bk, variant):
     """Every row-block variant (streamed runs of rows, row groups, banded) on
     rows of every length class: empty, short, up to the staging buffer, long
-    (the second launch), mixed within one 32-row block and its 16-row halves.
+    (the second launch), and blocks that split into several runs.
     The 2000 columns fit the banded variant's shared-memory band."""
     rng = np.random.default_rng(40 + variant)
     lens = rng.choice([0, 1, 3, 7, 8, 9, 15, 16, 17, 40, 100, 255, 256, 257, 600], size=203)

@@ -46,10 +46,10 @@ METRIC = "LP solves/s at rel KKT 1e-6"
 N_LP = 256
 EPS = 1e-6
 # DRAM bytes per algorithmic byte of engine_persistent on this batch, from one
-# ncu capture of the second 256-step launch of
-# `bench.py --workload engine-steps --iters 512`: dram__bytes_read.sum +
-# dram__bytes_write.sum = 93.34 GB against 87.55 GB of algorithmic bytes.
-TRAFFIC_PER_ALGORITHMIC_BYTE = 93.34 / 87.55
+# ncu capture of the first 256-step launch of
+# `bench.py --workload engine-steps --iters 300`: dram__bytes_read.sum +
+# dram__bytes_write.sum = 80.39 GB against 75.90 GB of algorithmic bytes.
+TRAFFIC_PER_ALGORITHMIC_BYTE = 80.39 / 75.90
 
 
 def load_peaks():
@@ -567,15 +567,18 @@ def _sync_events(torch):
 
 def run_blend(args):
     """Single large LP (200k x 600k, 3M nnz, 720-period blending plan,
-    log-uniform values): float64 vs float32-SpMV iteration throughput and the
-    engine kernel's achieved bandwidth over a fixed number of iterations."""
+    log-uniform values; ``--scale`` shrinks it): float64 vs float32-SpMV
+    iteration throughput, the engine kernel's achieved bandwidth, and the
+    KKT history, run to rel KKT 1e-6 or ``--iters`` iterations."""
     import torch
     from sovereign_moe_b200.batch import BatchEngine
     from sovereign_moe_b200.pdlp import PDLPParams
     from sovereign_moe_b200.workloads import blending_plan
-    k = blending_plan(seed=0)
+    sc = args.scale
+    k = blending_plan(seed=0, m=int(200_000 * sc), n=int(600_000 * sc),
+                      periods=max(1, int(720 * sc)), coupling=max(1, int(30 * sc)))
     peak, kind = load_peaks()
-    out = {"workload": "blending_plan_200k_x_600k", "nnz": int(k.problem.nnz),
+    out = {"workload": f"blending_plan_{k.problem.A.m}_x_{k.problem.A.n}", "nnz": int(k.problem.nnz),
            "iterations": args.iters}
     for prec in ("fp64", "fp32"):
         p = PDLPParams(device="gpu", eps_abs=1e-6, eps_rel=1e-6, max_iter=args.iters,
@@ -593,7 +596,13 @@ def run_blend(args):
                 if a == 0:
                     break
             r = eng.poll(slot)
+            sol = eng.fetch(slot)
+            h = sol.log
+            pick = sorted(set(list(range(0, len(h), max(1, len(h) // 8))) + [len(h) - 1])) if h else []
             out[prec] = {"ms": ms, "iters": int(r.iterations), "status": int(r.status),
+                         "kkt_history": [{"k": h[i][0], "primal_res": h[i][1], "dual_res": h[i][2],
+                                          "gap": h[i][3], "primal_obj": h[i][4]} for i in pick],
+                         "rel_obj_err_vs_known": abs(sol.objective - k.f_star) / max(1.0, abs(k.f_star)),
                          "us_per_iter": 1000.0 * ms / max(1, r.iterations),
                          "achieved_GBps": by / ms / 1e6 if ms else 0.0,
                          "frac_of_measured_hbm": by / ms / 1e6 / peak if ms else 0.0}

@@ -64,14 +64,30 @@ __device__ __forceinline__ double merit(double omega, double p, double d, double
 // false; its atomic, when it leaves the group, counts them all and releases
 // their partials together (every partial is written by lane 0, the lane that
 // issues the atomic).  Which warp completes a group changes nothing in the
-// sums, whose order is the tile order.
+// sums, whose order is the tile order.  A pass with nothing to reduce (a
+// normal iteration's A^T pass only advances the state machine) skips the
+// group level: warps count their tiles straight into the instance's counter
+// (n_tiles on this side), which takes one atomic round trip off the pass's
+// last warp.  Every tile of an instance in one pass has the same mode, so a
+// pass uses the counter one way only.
 __device__ __forceinline__ bool warp_finish(const EngineArgs& A, const Tile& t, int side,
-                                            int g_first, int g_last, bool need_red, Ops ops,
-                                            double* res, int lane, BulkPhase& ph) {
+                                            int g_first, int g_last, int n_tiles, bool need_red,
+                                            Ops ops, double* res, int lane, BulkPhase& ph) {
   ph.pend += 1;
   if (!ph.flush) return false;
   const unsigned done = ph.pend;
   ph.pend = 0;
+  if (!need_red) {
+    unsigned fin = 0;
+    __syncwarp();
+    if (lane == 0)
+      fin = atom_add_acq_rel(A.counters + 2 * t.inst + side, done) + done == (unsigned)n_tiles;
+    fin = __shfl_sync(kFull, fin, 0);
+    if (!fin) return false;
+    if (lane == 0) A.counters[2 * t.inst + side] = 0;
+    __syncwarp();
+    return true;
+  }
   const int g = t.group;
   const int2 gt = A.group_tiles[g];
   const double* tp = A.partials + (side ? (size_t)A.n_rtiles * kNP : 0);
@@ -420,7 +436,8 @@ __device__ void hot_rtile(const EngineArgs& A, const Tile& t, int ti, const Inst
   }
   if (!need_fin) return;
   double res[kNP];
-  if (warp_finish(A, t, 0, I.rg_begin, I.rg_end, need_red, ops, res, lane, ph)) {
+  if (warp_finish(A, t, 0, I.rg_begin, I.rg_end, I.rt_end - I.rt_begin, need_red, ops, res,
+                  lane, ph)) {
     if (lane == 0) r_finish(A, I, S, rmode, res);
     __syncwarp();
   }
@@ -498,7 +515,8 @@ __device__ void hot_ctile(const EngineArgs& A, const Tile& t, int ti, const Inst
     }
   }
   double res[kNP];
-  if (warp_finish(A, t, 1, I.cg_begin, I.cg_end, need_red, ops, res, lane, ph)) {
+  if (warp_finish(A, t, 1, I.cg_begin, I.cg_end, I.ct_end - I.ct_begin, need_red, ops, res,
+                  lane, ph)) {
     if (lane == 0) c_finish(A, I, S, cmode, res);
     __syncwarp();
   }
@@ -800,7 +818,8 @@ __device__ void process_rtile(const EngineArgs& A, const Tile t, int ti, WarpSme
   }
   if (!need_fin) return;
   double res[kNP];
-  if (warp_finish(A, t, 0, I.rg_begin, I.rg_end, need_red, ops, res, lane, ph)) {
+  if (warp_finish(A, t, 0, I.rg_begin, I.rg_end, I.rt_end - I.rt_begin, need_red, ops, res,
+                  lane, ph)) {
     if (lane == 0) r_finish(A, I, S, rmode, res);
     __syncwarp();
   }
@@ -1297,7 +1316,8 @@ __device__ void process_ctile(const EngineArgs& A, const Tile t, int ti, WarpSme
     }
   }
   double res[kNP];
-  if (warp_finish(A, t, 1, I.cg_begin, I.cg_end, need_red, ops, res, lane, ph)) {
+  if (warp_finish(A, t, 1, I.cg_begin, I.cg_end, I.ct_end - I.ct_begin, need_red, ops, res,
+                  lane, ph)) {
     if (lane == 0) c_finish(A, I, S, cmode, res);
     __syncwarp();
   }

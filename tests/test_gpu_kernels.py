@@ -147,6 +147,23 @@ def test_streamed_rows_equal_oracle_bitwise(bk, variant):
     assert np.array_equal(got, po.spmv(A.rp, A.ri, A.rx, x))
 
 
+@pytest.mark.parametrize("variant", [1, 2, 3])
+def test_spmv_rows_summed_in_place_and_by_the_second_launch(bk, variant):
+    """Rows of more than 256 entries are summed by the second launch from a
+    list kept per stream; rows at and around that bound and far beyond it,
+    beside short and empty rows, twice in a row on the same stream."""
+    rng = np.random.default_rng(60 + variant)
+    lens = [0, 4096, 4097, 9000, 5, 300, 257, 0, 12_000, 3] * 3
+    m, n = len(lens), 15_000
+    rows = np.repeat(np.arange(m), lens)
+    cols = np.concatenate([rng.choice(n, size=k, replace=False) for k in lens])
+    A = SparseMatrix.from_triplets(rows, cols, rng.standard_normal(rows.size), m, n)
+    for seed in (0, 1):
+        x = np.random.default_rng(seed).standard_normal(n)
+        exp = po.spmv(A.rp, A.ri, A.rx, x)
+        np.testing.assert_allclose(_spmv_ex(bk, variant, A, x), exp, rtol=1e-12, atol=1e-12)
+
+
 def test_banded_variant_on_a_band_wider_than_shared_memory(bk):
     """Blocks whose index span exceeds the band gather from global memory;
     a banded matrix whose blocks fit stages them; both agree with the oracle."""

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define PDLP_ABI_VERSION 4
+#define PDLP_ABI_VERSION 5
 
 /* ---- error codes ------------------------------------------------------- */
 #define PDLP_OK                   0
@@ -416,6 +416,90 @@ int pdlp_bnr_step_sizes(pdlp_bnr* b, int32_t K, double* eta, double* omega);
  * The result equals pdlp_dot's up to rounding (a different, but fixed,
  * summation tree). */
 int pdlp_dot_noalloc(int64_t n, const double* a, const double* b, double* out, void* stream);
+
+/* ---- crossover to a basis (host) ---------------------------------------
+ * Turns a PDLP point into an optimal basic solution, for ranging and warm
+ * starts: sovopt's src/sovopt/lp/crossover.py (basis_from_point, crossover).
+ * Both calls run on the host cores and take a problem with memory
+ * PDLP_MEM_HOST; c is minimised and `sense` is ignored (the caller negates c
+ * and y for a maximisation, as crossover.py:206-211 does).  Statuses over
+ * [x ; s] (n structurals, then one logical per row, bounded by the row's
+ * bounds), with the values of src/sovopt/lp/basis.py:75-79: */
+#define PDLP_BASIC     0
+#define PDLP_AT_LOWER  1
+#define PDLP_AT_UPPER  2
+#define PDLP_FREE      3
+#define PDLP_FIXED     4
+#define PDLP_STATUS_UNBOUNDED 2
+
+typedef struct pdlp_crossover_info {
+    int32_t placed;          /* structurals pushed into the basis             */
+    int32_t candidates;      /* structurals offered (free, then by score)     */
+    int32_t rejected;        /* offered but dependent on those already in     */
+    int32_t factorizations;
+    int32_t repairs;         /* dependent columns swapped for logicals at a
+                                refactorisation (0 by construction)           */
+    int32_t reserved;
+    double seconds;
+} pdlp_crossover_info;
+
+/* basis_from_point (crossover.py:80-187): scores every variable of [x ; s]
+ * by its distance to the nearest bound relative to its range (less 1e-9
+ * |d_j| with d = c - A'y, or nothing when y is NULL), offers the free
+ * structurals and then those scoring above 1e-9 by decreasing score, and
+ * pushes each into the basis (starting from the all-logical one) on the
+ * largest |B^-1 M_j| entry in a row still holding its logical, skipping it
+ * when that entry is at most pivot_tol.  status_out (n + m) gets exactly m
+ * PDLP_BASIC entries; the rest rest on their nearest bound (PDLP_FIXED when
+ * the bounds are within tol_fixed * max(1, |lb|)).  The reference passes
+ * tol_fixed = 1e-12 and pivot_tol = max(SimplexParams.pivot_tol, 1e-7). */
+int pdlp_basis_from_point(const pdlp_problem_desc* prob, const double* x, const double* y,
+                          double tol_fixed, double pivot_tol, uint8_t* status_out,
+                          pdlp_crossover_info* info);
+
+/* SimplexParams (src/sovopt/lp/simplex.py:94-196): the fields this simplex
+ * uses, with the same defaults. */
+typedef struct pdlp_simplex_params {
+    double feas_tol, opt_tol, pivot_tol;     /* 1e-7 each                     */
+    int64_t max_iter;                        /* 1,000,000                     */
+    double time_limit;                       /* 300 s                         */
+    int32_t refactor_freq;                   /* 150 pivots between LUs        */
+    int32_t reserved;
+} pdlp_simplex_params;
+
+typedef struct pdlp_simplex_info {
+    int32_t status;          /* PDLP_STATUS_*                                 */
+    int32_t phase;           /* the phase it ended in (1 or 2)                */
+    int64_t iterations;      /* pivots plus bound flips                       */
+    int64_t phase1_iterations, bound_flips, degenerate_pivots;
+    int64_t dual_iterations;   /* pivots of the dual simplex                 */
+    int64_t cost_shifts;       /* costs shifted to make a start dual feasible */
+    int32_t factorizations, repairs;
+    double objective;        /* c'x of the returned point                     */
+    double primal_infeasibility, dual_infeasibility;
+    int64_t lu_nnz;
+    double seconds;
+} pdlp_simplex_info;
+
+int pdlp_simplex_default_params(pdlp_simplex_params* params);
+
+/* The revised simplex that finishes a crossover (the role of
+ * src/sovopt/lp/simplex.py:1181-1374 in crossover.py:213), on a copy of the
+ * LP scaled by powers of two.  From warm_status when it has exactly m
+ * PDLP_BASIC entries, else from the all-logical basis: a primal feasible
+ * start goes to the primal simplex; any other start is made dual feasible
+ * (boxed nonbasics moved to the bound their reduced cost wants, the other
+ * costs shifted) and runs the bounded dual simplex to primal feasibility,
+ * then, with the true costs, the primal simplex (Dantzig pricing, Harris
+ * ratio test with bound flips, Bland's rule after 50 degenerate pivots in a
+ * row).  A dual ray is confirmed by a composite primal phase 1 before
+ * INFEASIBLE is returned.  It returns OPTIMAL only once fresh factors show
+ * the basis primal feasible to feas_tol and dual feasible to opt_tol.  Writes x
+ * (n), y (m, B^-T c_B), d (n, c - A'y, 0 on basic columns) and the final
+ * basis_status (n + m).  params NULL: defaults. */
+int pdlp_simplex_solve(const pdlp_problem_desc* prob, const pdlp_simplex_params* params,
+                       const uint8_t* warm_status, double* x, double* y, double* d,
+                       uint8_t* basis_status, pdlp_simplex_info* info);
 
 #ifdef __cplusplus
 }

@@ -94,6 +94,35 @@ class Tuning(ctypes.Structure):
                 ("default_us_per_iteration", ctypes.c_double)]
 
 
+class CrossoverInfo(ctypes.Structure):
+    _fields_ = [("placed", ctypes.c_int32), ("candidates", ctypes.c_int32),
+                ("rejected", ctypes.c_int32), ("factorizations", ctypes.c_int32),
+                ("repairs", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("seconds", ctypes.c_double)]
+
+
+class SimplexParamsC(ctypes.Structure):
+    _fields_ = [("feas_tol", ctypes.c_double), ("opt_tol", ctypes.c_double),
+                ("pivot_tol", ctypes.c_double), ("max_iter", ctypes.c_int64),
+                ("time_limit", ctypes.c_double), ("refactor_freq", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+class SimplexInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("phase", ctypes.c_int32),
+                ("iterations", ctypes.c_int64), ("phase1_iterations", ctypes.c_int64),
+                ("bound_flips", ctypes.c_int64), ("degenerate_pivots", ctypes.c_int64),
+                ("dual_iterations", ctypes.c_int64), ("cost_shifts", ctypes.c_int64),
+                ("factorizations", ctypes.c_int32), ("repairs", ctypes.c_int32),
+                ("objective", ctypes.c_double), ("primal_infeasibility", ctypes.c_double),
+                ("dual_infeasibility", ctypes.c_double), ("lu_nnz", ctypes.c_int64),
+                ("seconds", ctypes.c_double)]
+
+
+# basis statuses (include/pdlp_b200.h; sovopt lp/basis.py:75-79)
+BASIC, AT_LOWER, AT_UPPER, FREE, FIXED = 0, 1, 2, 3, 4
+
+
 # Every symbol include/pdlp_b200.h declares, with its argument types.
 _i32, _i64, _d = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
 SIGNATURES = {
@@ -152,6 +181,11 @@ SIGNATURES = {
                             ctypes.c_int),
     "pdlp_tune_cache_put": ([ctypes.POINTER(TuneKey), ctypes.POINTER(Tuning)], ctypes.c_int),
     "pdlp_tune_cache_clear": ([], None),
+    "pdlp_basis_from_point": ([ctypes.POINTER(ProblemDesc), _c_p, _c_p, _d, _d, _c_p,
+                               ctypes.POINTER(CrossoverInfo)], ctypes.c_int),
+    "pdlp_simplex_default_params": ([ctypes.POINTER(SimplexParamsC)], ctypes.c_int),
+    "pdlp_simplex_solve": ([ctypes.POINTER(ProblemDesc), ctypes.POINTER(SimplexParamsC), _c_p,
+                            _c_p, _c_p, _c_p, _c_p, ctypes.POINTER(SimplexInfo)], ctypes.c_int),
 }
 
 _LIB = None

@@ -9,6 +9,13 @@ bound violation), and with ``--out`` writes the same JSON payload:
 ``x`` and ``y`` (lists, or name-keyed objects with ``--named``).  That file
 is what the reference's verifier (``bench/verify.py:279-318``) reads.
 
+``--crossover`` crosses the PDLP point over to an optimal basis
+(``crossover.py``; the reference's ``cli.py:167-182`` with the parameters it
+passes: feas_tol = opt_tol = max(tol, 1e-9)).  In the reference the
+``--method pdlp`` branch returns before the crossover branch is reached
+(``cli.py:163-166``), so there the flag takes effect only with ``--method
+ipm``; here it applies to the PDLP solve.
+
 Extensions of this build: ``--precision fp32`` (float32 sparse products) and
 ``--refine`` (float32 inner solves with float64 iterative refinement to
 ``--tol``).  Only ``--method pdlp`` exists here; the reference's other
@@ -70,6 +77,12 @@ def cmd_solve(a) -> int:
         sol = solve_refined(prob, params, target=a.tol)
     else:
         sol = solve_pdlp(prob, params)
+    if a.crossover and sol.x is not None:
+        from .crossover import crossover
+        from .simplex import SimplexParams
+        sol = crossover(prob, sol.x, sol.y,
+                        SimplexParams(time_limit=a.time_limit, feas_tol=max(a.tol, 1e-9),
+                                      opt_tol=max(a.tol, 1e-9), verbose=a.verbose))
     dt = time.perf_counter() - t
     print()
     print(f"  status      {sol.status.name}")
@@ -128,6 +141,8 @@ def main(argv=None) -> int:
                    help="key x and y by column and row names in the JSON")
     p.add_argument("--print-solution", type=int, default=0, metavar="N")
     p.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
+    p.add_argument("--crossover", action="store_true",
+                   help="cross the PDLP point over to an optimal simplex basis")
     p.add_argument("--refine", action="store_true",
                    help="float32 inner solves, float64 iterative refinement to --tol")
     p.add_argument("-v", "--verbose", action="store_true")

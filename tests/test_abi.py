@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_defaults_match_reference_params():
     lib = _lib.load()
-    assert lib.pdlp_abi_version() == 4
+    assert lib.pdlp_abi_version() == 5
     p = _lib.Params()
     lib.pdlp_params_default(ctypes.byref(p))
     ref = PDLPParams()
@@ -135,3 +135,29 @@ def test_tuning_cache_api_without_a_gpu(tmp_path):
     assert tuning.load(path) == 1
     assert tuning.entries() == e
     tuning.clear()
+
+
+def test_struct_sizes_equal_the_compiled_header(tmp_path):
+    """Every struct the header declares has the size ctypes gives it, as the
+    host C compiler lays it out."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    structs = {"pdlp_problem_desc": _lib.ProblemDesc, "pdlp_params": _lib.Params,
+               "pdlp_result": _lib.Result, "pdlp_batch_config": _lib.BatchConfig,
+               "pdlp_tune_key": _lib.TuneKey, "pdlp_tuning": _lib.Tuning,
+               "pdlp_crossover_info": _lib.CrossoverInfo,
+               "pdlp_simplex_params": _lib.SimplexParamsC,
+               "pdlp_simplex_info": _lib.SimplexInfo}
+    src = tmp_path / "sizes.c"
+    src.write_text('#include <stdio.h>\n#include "pdlp_b200.h"\nint main(void) {\n' +
+                   "".join(f'  printf("{k} %zu\\n", sizeof({k}));\n' for k in structs) +
+                   "  return 0;\n}\n")
+    exe = tmp_path / "sizes"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    got = dict((k, int(v)) for k, v in (line.split() for line in out.splitlines()))
+    assert got == {k: ctypes.sizeof(v) for k, v in structs.items()}

@@ -699,11 +699,14 @@ def run_spmv(args):
         flush.zero_()
         flush.sum(dtype=torch.int64)
 
-    mats = [("blending_plan_200k_x_600k", blending_plan(seed=0).problem)]
+    mats = []
+    if args.matrix in ("all", "blending"):
+        mats.append(("blending_plan_200k_x_600k", blending_plan(seed=0).problem))
     sc = args.scale
-    mats.append((f"power_law_{int(1e6 * sc)}x{int(3e6 * sc)}",
-                 power_law(seed=0, m=int(1_000_000 * sc), n=int(3_000_000 * sc),
-                           nnz=int(10_000_000 * sc)).problem))
+    if args.matrix in ("all", "power_law"):
+        mats.append((f"power_law_{int(1e6 * sc)}x{int(3e6 * sc)}",
+                     power_law(seed=0, m=int(1_000_000 * sc), n=int(3_000_000 * sc),
+                               nnz=int(10_000_000 * sc)).problem))
     names = {_lib.PDLP_SPMV_STREAMED: "streamed", _lib.PDLP_SPMV_ROW_GROUPS: "row_groups",
              _lib.PDLP_SPMV_BANDED: "banded"}
     rows = []
@@ -742,18 +745,53 @@ def run_spmv(args):
                     return statistics.median(times)
 
                 per = {names[v]: timed(v) for v in names}
+                # the planned kernel: the pattern analysed once, then one
+                # persistent launch per product
+                plan = ctypes.c_void_p()
+                _lib.check(lib.pdlp_spmv_plan_create(int(r), int(c), rp.data_ptr(), ri.data_ptr(),
+                                                     stream.cuda_stream, ctypes.byref(plan)))
+                pinfo = _lib.SpmvPlanInfo()
+                _lib.check(lib.pdlp_spmv_plan_get_info(plan, ctypes.byref(pinfo)))
+                prun = lib.pdlp_spmv_plan_run_f64 if prec == "fp64" else lib.pdlp_spmv_plan_run_f32
+
+                def timed_plan():
+                    call = lambda: _lib.check(prun(plan, rx.data_ptr(), x.data_ptr(),  # noqa: E731
+                                                   y.data_ptr(), stream.cuda_stream))
+                    for _ in range(3):
+                        call()
+                    times = []
+                    for _ in range(args.steps * 10):
+                        flush_l2()
+                        e0, e1 = _sync_events(torch)
+                        e0.record()
+                        call()
+                        e1.record()
+                        e1.synchronize()
+                        times.append(e0.elapsed_time(e1))
+                    return statistics.median(times)
+
+                per["planned"] = timed_plan()
+                _lib.check(lib.pdlp_spmv_plan_status(plan, stream.cuda_stream))
+                lib.pdlp_spmv_plan_destroy(plan)
                 best = ctypes.c_int32(0)
                 tms = (ctypes.c_double * 3)()
                 _lib.check(tune(int(r), rp.data_ptr(), ri.data_ptr(), rx.data_ptr(), x.data_ptr(),
                                 y.data_ptr(), stream.cuda_stream, 10, ctypes.byref(best), tms))
                 ms = per[names[best.value]]
+                pms = per["planned"]
                 rows.append({"matrix": name, "product": side, "dtype": prec, "rows": int(r),
                              "nnz": nnz, "algorithmic_bytes": algo,
                              "ms_per_variant": per, "tuned_variant": names[best.value],
                              "tuner_ms_warm_l2": {"streamed": tms[0], "row_groups": tms[1],
                                                   "banded": tms[2]},
                              "ms": ms, "GBps": algo / ms / 1e6,
-                             "frac_of_measured_hbm": algo / ms / 1e6 / peak})
+                             "frac_of_measured_hbm": algo / ms / 1e6 / peak,
+                             "planned": {"ms": pms, "GBps": algo / pms / 1e6,
+                                         "frac_of_measured_hbm": algo / pms / 1e6 / peak,
+                                         "plan_seconds": pinfo.seconds, "tiles": pinfo.tiles,
+                                         "banded_tiles": pinfo.banded_tiles,
+                                         "entries_in_band": pinfo.entries_in_band,
+                                         "huge_rows": pinfo.huge_rows}})
                 del rp, ri, rx, x, y
     print(json.dumps({"metric": "SpMV HBM GB/s", "unit": "GB/s", "results": rows,
                       "peak_GBps": peak, "peak_source": kind,
@@ -988,6 +1026,8 @@ def main():
                     help="batch: the headline metric; the others print auxiliary lines")
     ap.add_argument("--iters", type=int, default=2000)
     ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--matrix", default="all", choices=["all", "blending", "power_law"],
+                    help="matrices of --workload spmv")
     ap.add_argument("--time-limit", type=float, default=600.0)
     ap.add_argument("--rate", type=float, default=200.0)
     ap.add_argument("--count", type=int, default=200)

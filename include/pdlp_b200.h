@@ -349,6 +349,54 @@ int pdlp_spmv_tune_f64(int32_t m, const int64_t* rp, const int32_t* ri, const do
 int pdlp_spmv_tune_f32(int32_t m, const int64_t* rp, const int32_t* ri, const float* rx,
                        const float* x, float* y, void* stream, int32_t reps,
                        int32_t* best_variant, double* ms_per_variant);
+/* Planned SpMV: y = A x on a fixed sparsity pattern, analysed once
+ * (backend.py:373-384 on the matrix the PDHG loop multiplies at every
+ * iteration).  pdlp_spmv_plan_create copies rp and ri to the host (it
+ * synchronises `stream`), checks them (non-decreasing pointers, 0 <= index <
+ * n_cols), cuts the rows into tiles of at most 512 rows and 2048 entries, and
+ * gives each tile a window of at most 3072 columns holding most of its indices
+ * plus a halo of up to 32 further columns (its most used outside the window).
+ * The plan keeps its own copy of the pattern on the device (rp and ri may be
+ * freed after the call); the values rx are passed to each run and may change.
+ * pdlp_spmv_plan_run_* launches one persistent kernel: per SM a copy warp
+ * streams tiles (row pointers, indices, values and the x window) into a ring
+ * of shared-memory stages with bulk asynchronous copies, a halo warp gathers
+ * the halo into the stage, and sixteen consumer warps sum the rows from shared
+ * memory; an entry in neither window nor halo gathers x from global memory.
+ * Rows of at most 64 entries are summed by one lane in storage order
+ * (bit-identical to the reference's CPU kernel); longer rows by a warp,
+ * lane-strided then a xor butterfly.  rx and x must be 16-byte aligned (as
+ * cudaMalloc and torch allocations are).  When fewer than half the entries
+ * fall in a window or halo, a run is the row-block kernel instead
+ * (pdlp_spmv_ex_* with PDLP_SPMV_STREAMED on the plan's copy; no alignment
+ * rule).  Asynchronous; repeated runs give the same bits.  A wait inside the
+ * kernel that runs out (1 s) records PDLP_ERR_BARRIER_TIMEOUT, which
+ * pdlp_spmv_plan_status returns (and clears) after synchronising `stream`. */
+typedef struct pdlp_spmv_plan pdlp_spmv_plan;
+#define PDLP_SPMV_PLAN_TILES     0
+#define PDLP_SPMV_PLAN_STREAMED  1
+typedef struct {
+  int32_t tiles;             /* tiles of rows */
+  int32_t banded_tiles;      /* tiles that stage an x window */
+  int32_t huge_rows;         /* rows over 2048 entries (read from global memory) */
+  int32_t ctas;              /* CTAs of a run (one per SM at most) */
+  int32_t kernel;            /* PDLP_SPMV_PLAN_TILES, or PDLP_SPMV_PLAN_STREAMED when fewer
+                                than half the entries are staged: a run is then
+                                pdlp_spmv_ex_* with PDLP_SPMV_STREAMED */
+  int32_t reserved;
+  int64_t entries;           /* nnz */
+  int64_t entries_in_band;   /* entries whose x is staged (window or halo) */
+  double seconds;            /* host time of pdlp_spmv_plan_create */
+} pdlp_spmv_plan_info;
+int pdlp_spmv_plan_create(int32_t m, int32_t n_cols, const int64_t* rp, const int32_t* ri,
+                          void* stream, pdlp_spmv_plan** out);
+int pdlp_spmv_plan_run_f64(pdlp_spmv_plan* plan, const double* rx, const double* x, double* y,
+                           void* stream);
+int pdlp_spmv_plan_run_f32(pdlp_spmv_plan* plan, const float* rx, const float* x, float* y,
+                           void* stream);
+int pdlp_spmv_plan_get_info(const pdlp_spmv_plan* plan, pdlp_spmv_plan_info* out);
+int pdlp_spmv_plan_status(pdlp_spmv_plan* plan, void* stream);
+void pdlp_spmv_plan_destroy(pdlp_spmv_plan* plan);
 /* Y = A X, X dense (ncols, k) row-major, batch index fastest (backend.py:386-400) */
 int pdlp_spmm_f64(int32_t m, int32_t k, const int64_t* rp, const int32_t* ri,
                   const double* rx, const double* X, double* Y, void* stream);

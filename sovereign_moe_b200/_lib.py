@@ -29,6 +29,8 @@ PDLP_SPMV_AUTO = 0
 PDLP_SPMV_STREAMED = 1
 PDLP_SPMV_ROW_GROUPS = 2
 PDLP_SPMV_BANDED = 3
+PDLP_SPMV_PLAN_TILES = 0
+PDLP_SPMV_PLAN_STREAMED = 1
 
 PDLP_STATUS_RUNNING = -1
 PDLP_SLOT_FREE = -2
@@ -94,6 +96,14 @@ class Tuning(ctypes.Structure):
                 ("default_us_per_iteration", ctypes.c_double)]
 
 
+class SpmvPlanInfo(ctypes.Structure):
+    _fields_ = [("tiles", ctypes.c_int32), ("banded_tiles", ctypes.c_int32),
+                ("huge_rows", ctypes.c_int32), ("ctas", ctypes.c_int32),
+                ("kernel", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("entries", ctypes.c_int64), ("entries_in_band", ctypes.c_int64),
+                ("seconds", ctypes.c_double)]
+
+
 class CrossoverInfo(ctypes.Structure):
     _fields_ = [("placed", ctypes.c_int32), ("candidates", ctypes.c_int32),
                 ("rejected", ctypes.c_int32), ("factorizations", ctypes.c_int32),
@@ -157,6 +167,12 @@ SIGNATURES = {
                             _c_p], ctypes.c_int),
     "pdlp_spmv_tune_f32": ([_i32, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _i32, ctypes.POINTER(_i32),
                             _c_p], ctypes.c_int),
+    "pdlp_spmv_plan_create": ([_i32, _i32, _c_p, _c_p, _c_p, ctypes.POINTER(_c_p)], ctypes.c_int),
+    "pdlp_spmv_plan_run_f64": ([_c_p, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
+    "pdlp_spmv_plan_run_f32": ([_c_p, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
+    "pdlp_spmv_plan_get_info": ([_c_p, ctypes.POINTER(SpmvPlanInfo)], ctypes.c_int),
+    "pdlp_spmv_plan_status": ([_c_p, _c_p], ctypes.c_int),
+    "pdlp_spmv_plan_destroy": ([_c_p], None),
     "pdlp_spmm_f64": ([_i32, _i32, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p], ctypes.c_int),
     "pdlp_primal_step": ([_i32, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _d, _c_p], ctypes.c_int),
     "pdlp_dual_step": ([_i32, _c_p, _c_p, _c_p, _c_p, _c_p, _d, _c_p], ctypes.c_int),

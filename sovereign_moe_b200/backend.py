@@ -17,12 +17,58 @@ import numpy as np
 
 from . import _lib
 
-__all__ = ["Backend", "get_backend", "gpu_selftest"]
+__all__ = ["Backend", "SpmvPlan", "get_backend", "gpu_selftest"]
 
 
 def _torch():
     import torch
     return torch
+
+
+class SpmvPlan:
+    """A planned ``y = A x`` on one sparsity pattern (``pdlp_spmv_plan_*``).
+
+    The reference multiplies by the same ``A`` and ``A^T`` at every PDHG
+    iteration (``backend.py:373-384``); the plan analyses the pattern once --
+    tiles of rows, each with the column window and halo its ``x`` gathers come
+    from -- and each ``run`` is one persistent kernel that streams the matrix
+    into shared memory.  The plan copies ``rp`` and ``ri`` (int64 / int32
+    device tensors); the values are passed to each run and may change.
+    """
+
+    def __init__(self, lib, rp, ri, m, n, stream):
+        self.lib = lib
+        self.m, self.n = int(m), int(n)
+        h = ctypes.c_void_p()
+        _lib.check(lib.pdlp_spmv_plan_create(self.m, self.n, rp.data_ptr(), ri.data_ptr(),
+                                             stream, ctypes.byref(h)))
+        self._h = h
+
+    def run(self, rx, x, out, stream):
+        torch = _torch()
+        fn = (self.lib.pdlp_spmv_plan_run_f32 if rx.dtype == torch.float32
+              else self.lib.pdlp_spmv_plan_run_f64)
+        _lib.check(fn(self._h, rx.data_ptr(), x.data_ptr(), out.data_ptr(), stream))
+        return out
+
+    def info(self) -> dict:
+        i = _lib.SpmvPlanInfo()
+        _lib.check(self.lib.pdlp_spmv_plan_get_info(self._h, ctypes.byref(i)))
+        return {f: getattr(i, f) for f, _ in i._fields_}
+
+    def status(self, stream) -> int:
+        return int(self.lib.pdlp_spmv_plan_status(self._h, stream))
+
+    def close(self):
+        if self._h:
+            self.lib.pdlp_spmv_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Backend:
@@ -101,6 +147,14 @@ class Backend:
         _lib.check(fn(int(variant), int(m), rp.data_ptr(), ri.data_ptr(), rx.data_ptr(),
                       x.data_ptr(), out.data_ptr(), self._stream()))
         return out
+
+    def spmv_plan(self, rp, ri, m, n) -> SpmvPlan:
+        """A plan for repeated ``A x`` on this pattern (synchronises the stream)."""
+        return SpmvPlan(self.lib, rp, ri, m, n, self._stream())
+
+    def spmv_planned(self, plan: SpmvPlan, rx, x, out):
+        """``out = A x`` through a plan made by :meth:`spmv_plan`."""
+        return plan.run(rx, x, out, self._stream())
 
     def spmm(self, rp, ri, rx, X, out, m, k_batch):
         """``out = A X``, ``X`` dense ``(n, k)`` row-major (``backend.py:386-400``)."""

@@ -19,7 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpdlp_b200.so")
-SOURCES = ["engine.cu", "kernels.cu", "bnr.cu", "crossover.cu"]
+SOURCES = ["engine.cu", "kernels.cu", "spmv_plan.cu", "bnr.cu", "crossover.cu"]
 HEADERS = ["common.cuh", "engine.cuh", "engine_device.cuh", "engine_passes.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

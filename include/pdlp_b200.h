@@ -338,7 +338,8 @@ int pdlp_spmv_ex_f64(int32_t variant, int32_t m, const int64_t* rp, const int32_
 int pdlp_spmv_ex_f32(int32_t variant, int32_t m, const int64_t* rp, const int32_t* ri,
                      const float* rx, const float* x, float* y, void* stream);
 /* The SpMV autotuner: times each variant on this matrix and these vectors
- * (one warm call, then `reps` calls, 0 = 10, with CUDA events on `stream`),
+ * (one warm call, then three interleaved rounds of `reps` calls, 0 = 10, with
+ * CUDA events on `stream`, each variant's fastest round counting),
  * writes y = A x, and returns the fastest variant in *best_variant and each
  * variant's milliseconds per call in ms_per_variant[3] (STREAMED, ROW_GROUPS,
  * BANDED; optional).  Synchronises the stream.  The reference has a fixed launch

@@ -377,9 +377,11 @@ int launch_spmv(int m, const int64_t* rp, const int* ri, const T* rx, const T* x
 }
 
 // The SpMV autotuner: times every variant of the row-block pass on the
-// caller's matrix and vectors (one warm call each, then `reps` calls bracketed
-// by CUDA events on the caller's stream) and returns the fastest.  Its cost is
-// a few dozen SpMVs; the caller keeps the choice for the matrix.
+// caller's matrix and vectors (one warm call each, then three interleaved
+// rounds of `reps` calls per variant bracketed by CUDA events on the caller's
+// stream, keeping each variant's fastest round, so that a passing change of
+// the GPU's state does not decide the choice) and returns the fastest.  Its
+// cost is about a hundred SpMVs; the caller keeps the choice for the matrix.
 template <typename T>
 int tune_spmv(int m, const int64_t* rp, const int* ri, const T* rx, const T* x, T* y,
               cudaStream_t st, int reps, int* best, double* ms_out) {
@@ -389,23 +391,32 @@ int tune_spmv(int m, const int64_t* rp, const int* ri, const T* rx, const T* x, 
   PDLP_CUDA(cudaEventCreate(&e0));
   const cudaError_t ce = cudaEventCreate(&e1);
   if (ce != cudaSuccess) { cudaEventDestroy(e0); return cuda_fail(ce, "cudaEventCreate"); }
+  constexpr int kRounds = 3;
   const int variants[3] = {SPMV_STREAMED, SPMV_ROW_GROUPS, SPMV_BANDED};
-  double best_ms = 0.0;
+  double per_ms[3] = {0.0, 0.0, 0.0};
   int rc = PDLP_OK;
+  for (int k = 0; k < 3 && rc == PDLP_OK; ++k) rc = launch_spmv<T>(m, rp, ri, rx, x, y, st, variants[k]);
+  for (int round = 0; round < kRounds && rc == PDLP_OK; ++round) {
+    for (int k = 0; k < 3 && rc == PDLP_OK; ++k) {
+      cudaEventRecord(e0, st);
+      for (int r = 0; r < reps && rc == PDLP_OK; ++r)
+        rc = launch_spmv<T>(m, rp, ri, rx, x, y, st, variants[k]);
+      cudaEventRecord(e1, st);
+      const cudaError_t se = cudaEventSynchronize(e1);
+      if (se != cudaSuccess) { rc = cuda_fail(se, "cudaEventSynchronize"); break; }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      const double per = (double)ms / reps;
+      if (round == 0 || per < per_ms[k]) per_ms[k] = per;
+    }
+  }
   *best = SPMV_STREAMED;
-  for (int k = 0; k < 3 && rc == PDLP_OK; ++k) {
-    rc = launch_spmv<T>(m, rp, ri, rx, x, y, st, variants[k]);
-    if (rc != PDLP_OK) break;
-    cudaEventRecord(e0, st);
-    for (int r = 0; r < reps && rc == PDLP_OK; ++r) rc = launch_spmv<T>(m, rp, ri, rx, x, y, st, variants[k]);
-    cudaEventRecord(e1, st);
-    const cudaError_t se = cudaEventSynchronize(e1);
-    if (se != cudaSuccess) { rc = cuda_fail(se, "cudaEventSynchronize"); break; }
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    const double per = (double)ms / reps;
-    if (ms_out) ms_out[k] = per;
-    if (k == 0 || per < best_ms) { best_ms = per; *best = variants[k]; }
+  if (rc == PDLP_OK) {
+    double best_ms = per_ms[0];
+    for (int k = 0; k < 3; ++k) {
+      if (ms_out) ms_out[k] = per_ms[k];
+      if (per_ms[k] < best_ms) { best_ms = per_ms[k]; *best = variants[k]; }
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -641,6 +641,36 @@ static void make_groups(std::vector<Tile>& tiles, int t0, int t1, int group_base
   }
 }
 
+// Iterations an instance is expected to need still, or a negative value when
+// nothing is known.  From its own progress once its checks span at least
+// kRateSpan iterations: the largest residual-to-tolerance ratio of the
+// termination test fell from r0 to its best rb over that span, so at the same
+// log-linear rate it needs log(rb) / rate more (an instance that has not
+// improved is taken to need as many again as it has done).  Otherwise from
+// the caller's estimate (pdlp_params.expected_iterations): an instance past
+// it is taken to need half as many iterations again.  The state copy is the
+// one read back after the last launch; it belongs to this instance once a
+// launch has counted iterations for it.
+static double expected_left(const pdlp_batch* b, int s) {
+  constexpr long long kRateSpan = 256;
+  const Slot& sl = b->slots[s];
+  const double d = (double)b->iters_before[s];
+  const State& hs = b->h_state[s];
+  if (d > 0.0 && hs.kkt_k_first > 0 && hs.kkt_k - hs.kkt_k_first >= kRateSpan &&
+      hs.kkt_best > 0.0) {
+    if (hs.kkt_best <= 1.0) return 64.0;
+    const double drop = std::log(hs.kkt_first / hs.kkt_best);
+    if (!(drop > 0.0)) return std::max(d, 64.0);
+    const double left = std::log(hs.kkt_best) * (double)(hs.kkt_k - hs.kkt_k_first) / drop;
+    return std::min(std::max(left, 64.0), 1e7);
+  }
+  if (sl.expected_iters > 0.0) {
+    const double e = sl.expected_iters;
+    return std::max(d < e ? e - d : 0.5 * d, 0.1 * e);
+  }
+  return -1.0;
+}
+
 // The block teams of a persistent launch.  With many running instances one
 // team of blocks steps them all.  With fewer (at most kTeamsFrom), each
 // instance gets its own team, so that no instance waits at a barrier for
@@ -649,8 +679,8 @@ static void make_groups(std::vector<Tile>& tiles, int t0, int t1, int group_base
 // cannot use go to the others (water-filling), and the blocks left by
 // rounding go to the largest remainders.  The weight is the instance's work
 // per iteration, times its expected remaining iterations when every running
-// instance carries an estimate (pdlp_params.expected_iterations): an
-// instance past its estimate is taken to need half as many iterations again.
+// instance has an estimate (expected_left: from its own progress, else from
+// pdlp_params.expected_iterations).
 // On the 256-LP batch (engine time per batch, with the idle rule of the
 // kernel), teams from 160, 200 and 256 running instances measured 585, 571
 // and 541 ms.  Returns the blocks of each running instance's team, in `run`
@@ -664,7 +694,11 @@ static std::vector<int> plan_teams(const pdlp_batch* b, const std::vector<int>& 
     return tblocks;
   const size_t T = run.size();
   bool hinted = true;
-  for (int s : run) hinted = hinted && b->slots[s].expected_iters > 0.0;
+  std::vector<double> left(T);
+  for (size_t k = 0; k < T; ++k) {
+    left[k] = expected_left(b, run[k]);
+    hinted = hinted && left[k] > 0.0;
+  }
   std::vector<double> w(T);
   std::vector<int> want(T);
   for (size_t k = 0; k < T; ++k) {
@@ -672,11 +706,7 @@ static std::vector<int> plan_teams(const pdlp_batch* b, const std::vector<int>& 
     double per = 0.0;
     for (double v : sl.rtw) per += v;
     for (double v : sl.ctw) per += v;
-    if (hinted) {
-      const double e = sl.expected_iters, d = (double)b->iters_before[run[k]];
-      const double left = d < e ? e - d : 0.5 * d;
-      per *= std::max(left, 0.1 * e);
-    }
+    if (hinted) per *= left[k];
     w[k] = per;
     const int tiles = std::max(sl.inst.rt_end - sl.inst.rt_begin, sl.inst.ct_end - sl.inst.ct_begin);
     want[k] = std::max(1, (tiles + kWarps - 1) / kWarps);    // one tile per warp

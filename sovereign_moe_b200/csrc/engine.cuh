@@ -136,6 +136,11 @@ struct State {
   double fin[5];            // (pu, du, gu, pobj, dobj) at OPTIMAL
   double objective;
   long long t_start_ns, t_end_ns;
+  // scheduling only: the largest residual-to-tolerance ratio of the
+  // termination test at the first check and the smallest since, with the
+  // iterations they were seen at (0: no check yet)
+  double kkt_first, kkt_best;
+  long long kkt_k_first, kkt_k;
 };
 
 struct Tile {

@@ -983,6 +983,15 @@ __device__ void c_finish(const EngineArgs& A, const Inst& I, State* S, int cmode
         schedule_final(S, PDLP_STATUS_OPTIMAL, use_avg ? 1 : 0);
         break;
       }
+      {   // how far from the test, for the host's team planning (no effect on the solve)
+        const double gtol = I.eps_abs + I.eps_rel * (fabs(pou) + fabs(dou));
+        const double r = fmax(pu / fmax(ptol, 1e-300), fmax(du / fmax(dtol, 1e-300), gu / fmax(gtol, 1e-300)));
+        if (isfinite(r) && r > 0.0) {
+          if (S->kkt_k_first == 0) { S->kkt_first = r; S->kkt_k_first = S->k; S->kkt_best = r; }
+          else if (r < S->kkt_best) S->kkt_best = r;
+          S->kkt_k = S->k;
+        }
+      }
       if (S->hist_len < I.hist_cap) {
         double* h = I.hist + 5 * (size_t)S->hist_len;
         h[0] = (double)S->k; h[1] = pu; h[2] = du; h[3] = gu; h[4] = pou;

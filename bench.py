@@ -328,10 +328,15 @@ class GpuArm:
             self.engine_ms += ms
             self.engine_bytes += by
             self.engine_launches += 1
+        # every LP's result, x, y and d, and the slots retired, with one
+        # synchronisation (pdlp_batch_collect_many)
+        n = len(slots)
+        res = (L.Result * n)()
+        ptrs = [(ct.c_void_p * n)(*[o[j].data_ptr() for o in outs]) for j in range(3)]
+        L.check(c.pdlp_batch_collect_many(self.eng.h, n, (ct.c_int32 * n)(*slots), res,
+                                          ptrs[0], ptrs[1], ptrs[2], mem, 1))
         statuses, starts, ends, self.per_lp = [], [], [], []
-        for s, (x, y, dd), k in zip(slots, outs, self.lps):
-            r = L.Result()
-            L.check(c.pdlp_batch_poll(self.eng.h, s, ct.byref(r)))
+        for r, k in zip(res, self.lps):
             statuses.append(r.status)
             starts.append(r.device_start_ns)
             ends.append(r.device_end_ns)
@@ -340,9 +345,6 @@ class GpuArm:
                                 "nnz": int(k.problem.A.nnz), "iterations": int(r.iterations),
                                 "restarts": int(r.restarts), "start_ns": int(r.device_start_ns),
                                 "end_ns": int(r.device_end_ns)})
-            L.check(c.pdlp_batch_fetch(self.eng.h, s, x.data_ptr(), y.data_ptr(), dd.data_ptr(),
-                                       None, mem))
-            L.check(c.pdlp_batch_retire(self.eng.h, s))
         first = min(starts)
         self.latencies = [admit_s + (e - first) * 1e-9 for e in ends]
         return statuses
@@ -364,13 +366,14 @@ class GpuArm:
             active = ct.c_int32(1)
             while active.value > 0:
                 L.check(c.pdlp_batch_step(h, 1 << 16, ct.byref(active)))
+            # result, x, y, d to pinned host buffers and the slot retired with
+            # one synchronisation, as the batched arm collects
             r = L.Result()
-            L.check(c.pdlp_batch_poll(h, s.value, ct.byref(r)))
+            one = lambda a: (ct.c_void_p * 1)(a.data_ptr())  # noqa: E731
+            L.check(c.pdlp_batch_collect_many(h, 1, (ct.c_int32 * 1)(s.value), ct.byref(r),
+                                              one(x), one(y), one(dd), L.PDLP_MEM_HOST, 1))
             if r.status != 0:
                 raise RuntimeError(f"one-at-a-time solve ended with status {r.status}")
-            L.check(c.pdlp_batch_fetch(h, s.value, x.data_ptr(), y.data_ptr(), dd.data_ptr(),
-                                       None, L.PDLP_MEM_HOST))
-            L.check(c.pdlp_batch_retire(h, s.value))
             service.append(time.perf_counter() - t0)
         return service
 

@@ -1701,13 +1701,8 @@ int pdlp_batch_last_timing(pdlp_batch* b, double* ms, double* iter_bytes, int64_
   return PDLP_OK;
 }
 
-int pdlp_batch_poll(pdlp_batch* b, int32_t slot, pdlp_result* r) {
-  if (!b || !r) return fail(PDLP_ERR_ARG, "NULL argument");
-  if (slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
-    return fail(PDLP_ERR_ARG, "no such slot");
-  State hs;
-  PDLP_CUDA(cudaMemcpyAsync(&hs, &b->d_state[slot], sizeof(State), cudaMemcpyDeviceToHost, b->stream));
-  PDLP_CUDA(cudaStreamSynchronize(b->stream));
+// The caller's view of one slot's state.
+static void result_of(const State& hs, pdlp_result* r) {
   std::memset(r, 0, sizeof(*r));
   const double nan = std::nan("");
   r->status = hs.status;
@@ -1728,6 +1723,58 @@ int pdlp_batch_poll(pdlp_batch* b, int32_t slot, pdlp_result* r) {
   r->device_seconds = hs.t_end_ns > hs.t_start_ns ? (hs.t_end_ns - hs.t_start_ns) * 1e-9 : 0.0;
   r->device_start_ns = hs.t_start_ns;
   r->device_end_ns = hs.t_end_ns;
+}
+
+int pdlp_batch_poll(pdlp_batch* b, int32_t slot, pdlp_result* r) {
+  if (!b || !r) return fail(PDLP_ERR_ARG, "NULL argument");
+  if (slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
+    return fail(PDLP_ERR_ARG, "no such slot");
+  State hs;
+  PDLP_CUDA(cudaMemcpyAsync(&hs, &b->d_state[slot], sizeof(State), cudaMemcpyDeviceToHost, b->stream));
+  PDLP_CUDA(cudaStreamSynchronize(b->stream));
+  result_of(hs, r);
+  return PDLP_OK;
+}
+
+int pdlp_batch_collect_many(pdlp_batch* b, int32_t n, const int32_t* slots, pdlp_result* results,
+                            double* const* x, double* const* y, double* const* d,
+                            int32_t memory, int32_t retire) {
+  if (!b || n < 0 || (n > 0 && !slots)) return fail(PDLP_ERR_ARG, "NULL argument");
+  if (memory != PDLP_MEM_HOST && memory != PDLP_MEM_DEVICE)
+    return fail(PDLP_ERR_ARG, "memory must be PDLP_MEM_HOST or PDLP_MEM_DEVICE");
+  std::vector<char> seen(b->slots.size(), 0);
+  for (int32_t i = 0; i < n; ++i) {
+    const int32_t slot = slots[i];
+    if (slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
+      return fail(PDLP_ERR_ARG, "no such slot: " + std::to_string(slot));
+    if (seen[slot]) return fail(PDLP_ERR_ARG, "slot listed twice: " + std::to_string(slot));
+    seen[slot] = 1;
+    if (b->slots[slot].running) return fail(PDLP_ERR_STATE, "slot is still running: " + std::to_string(slot));
+  }
+  if (n == 0) return PDLP_OK;
+  const cudaMemcpyKind k = memory == PDLP_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  cudaStream_t st = b->stream;
+  PDLP_CUDA(cudaMemcpyAsync(b->h_state, b->d_state, sizeof(State) * b->slots.size(),
+                            cudaMemcpyDeviceToHost, st));
+  for (int32_t i = 0; i < n; ++i) {
+    const Slot& sl = b->slots[slots[i]];
+    if (x && x[i] && sl.n) PDLP_CUDA(cudaMemcpyAsync(x[i], sl.inst.xout, sizeof(double) * sl.n, k, st));
+    if (y && y[i] && sl.m) PDLP_CUDA(cudaMemcpyAsync(y[i], sl.inst.yout, sizeof(double) * sl.m, k, st));
+    if (d && d[i] && sl.n) PDLP_CUDA(cudaMemcpyAsync(d[i], sl.inst.dout, sizeof(double) * sl.n, k, st));
+  }
+  PDLP_CUDA(cudaStreamSynchronize(st));
+  for (int32_t i = 0; i < n; ++i)
+    if (results) result_of(b->h_state[slots[i]], results + i);
+  if (retire) {
+    for (int32_t i = 0; i < n; ++i) {
+      Slot& sl = b->slots[slots[i]];
+      b->spare.push_back({sl.arena, sl.bytes});
+      b->bytes_spare += sl.bytes;
+      b->bytes_held -= sl.bytes;
+      sl = Slot();
+    }
+    b->dirty = true;
+  }
   return PDLP_OK;
 }
 

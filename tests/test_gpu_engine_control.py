@@ -193,3 +193,46 @@ def test_scheduling_hints_change_no_result(require_gpu):
         hinted = eng.solve_all(probs, P6, hints=hints)
     for a, b in zip(plain, hinted):
         _same(a, b)
+
+
+def test_collect_many_equals_poll_fetch_retire(require_gpu):
+    """``pdlp_batch_collect_many`` (results, x, y, d and retirement of many
+    finished slots with one synchronisation) gives the same bits as
+    ``pdlp_batch_poll`` + ``pdlp_batch_fetch`` per slot, retires the slots so
+    their arenas serve later admissions, and refuses a running, free or
+    repeated slot before copying anything."""
+    import ctypes
+    probs = [k.problem for k in uneven_batch(seed=31, count=5, m_lo=60, m_hi=900)]
+    with BatchEngine(max_slots=8) as eng:
+        slots, codes = eng.admit_many(probs, P6)
+        assert codes == [0] * 5
+        lib = eng.lib
+        n = len(slots)
+        arr = (ctypes.c_int32 * n)(*slots)
+        assert lib.pdlp_batch_collect_many(eng.h, n, arr, None, None, None, None,
+                                           _lib.PDLP_MEM_HOST, 0) == _lib.PDLP_ERR_STATE
+        eng.run()
+        ref = [eng.fetch(s) for s in slots]
+        polls = [eng.poll(s) for s in slots]
+        xs = [np.full(p.A.n, np.nan) for p in probs]
+        ys = [np.full(p.A.m, np.nan) for p in probs]
+        ds = [np.full(p.A.n, np.nan) for p in probs]
+        ptr = lambda vs: (ctypes.c_void_p * n)(*[v.ctypes.data for v in vs])  # noqa: E731
+        twice = (ctypes.c_int32 * 2)(slots[0], slots[0])
+        assert lib.pdlp_batch_collect_many(eng.h, 2, twice, None, None, None, None,
+                                           _lib.PDLP_MEM_HOST, 1) == _lib.PDLP_ERR_ARG
+        res = (_lib.Result * n)()
+        assert lib.pdlp_batch_collect_many(eng.h, n, arr, res, ptr(xs), ptr(ys), ptr(ds),
+                                           _lib.PDLP_MEM_HOST, 1) == 0
+        for i in range(n):
+            assert bytes(res[i]) == bytes(polls[i])
+            assert np.array_equal(xs[i], ref[i].x) and np.array_equal(ys[i], ref[i].y)
+            assert np.array_equal(ds[i], ref[i].reduced_costs)
+        # retired: the slots are free, and a new admission reuses an arena
+        assert lib.pdlp_batch_collect_many(eng.h, 1, (ctypes.c_int32 * 1)(slots[0]), None, None,
+                                           None, None, _lib.PDLP_MEM_HOST, 1) == _lib.PDLP_ERR_ARG
+        assert list(eng.statuses()[:8]).count(_lib.PDLP_SLOT_FREE) == 8
+        again, codes = eng.admit_many(probs[:2], P6)
+        assert codes == [0, 0]
+        eng.run()
+        _same(eng.fetch(again[0]), ref[0])

@@ -336,7 +336,9 @@ struct AdmitTasks {
   int* err;
 };
 
-__global__ void admission_check(AdmitTasks T) {
+// The checks of one admission: blockIdx.y picks the array (0, 1 pointers, 2, 3
+// indices, 4..10 values, costs and bounds), x-blocks stride over it.
+__device__ void admission_check_one(const AdmitTasks& T) {
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   switch (blockIdx.y) {
@@ -375,6 +377,42 @@ __global__ void admission_check(AdmitTasks T) {
         if (isnan(v) || (!allow_inf && isinf(v))) atomicOr(T.err, 2);
       }
       break;
+    }
+  }
+}
+
+// Every admission of one admit call in one launch: blockIdx.z picks it.
+__global__ void admission_check(const AdmitTasks* __restrict__ tasks) {
+  admission_check_one(tasks[blockIdx.z]);
+}
+
+// A piece of an admission's input copies: bytes from src to dst, or, with
+// src null, zeros.  The pieces of one admit call are copied by one launch
+// (device-resident inputs) instead of a copy call per array.
+struct CopyPiece {
+  char* dst;
+  const char* src;
+  long long bytes;
+};
+
+__global__ void __launch_bounds__(256) gather_copy(const CopyPiece* __restrict__ pieces, int n) {
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const CopyPiece pc = pieces[i];
+    const unsigned long long a = (unsigned long long)pc.dst | (unsigned long long)pc.src |
+                                 (unsigned long long)pc.bytes;
+    if ((a & 15ull) == 0) {
+      uint4* d = reinterpret_cast<uint4*>(pc.dst);
+      const uint4* sv = reinterpret_cast<const uint4*>(pc.src);
+      const long long w = pc.bytes / 16;
+      for (long long k = threadIdx.x; k < w; k += blockDim.x) d[k] = pc.src ? sv[k] : make_uint4(0, 0, 0, 0);
+    } else if ((a & 7ull) == 0) {
+      unsigned long long* d = reinterpret_cast<unsigned long long*>(pc.dst);
+      const unsigned long long* sv = reinterpret_cast<const unsigned long long*>(pc.src);
+      const long long w = pc.bytes / 8;
+      for (long long k = threadIdx.x; k < w; k += blockDim.x) d[k] = pc.src ? sv[k] : 0ull;
+    } else {
+      for (long long k = threadIdx.x; k < pc.bytes; k += blockDim.x)
+        pc.dst[k] = pc.src ? pc.src[k] : (char)0;
     }
   }
 }
@@ -522,6 +560,12 @@ struct pdlp_batch {
   State* h_init = nullptr;             // pinned: initial states, one per slot
   int64_t* h_ptrs = nullptr;           // pinned: device pointer arrays read for admission
   size_t cap_hptrs = 0;
+  CopyPiece* h_pieces = nullptr;       // pinned / device: an admit call's copy pieces
+  CopyPiece* d_pieces = nullptr;
+  size_t cap_pieces = 0;
+  AdmitTasks* h_tasks = nullptr;       // pinned / device: an admit call's device checks
+  AdmitTasks* d_tasks = nullptr;
+  size_t cap_tasks = 0;
   bool force_set = false;              // tuning runs: every admission takes `force`
   pdlp_tuning force{};
   int force_blocks = 0;                // tuning runs: the one team's block count (0: free)
@@ -601,12 +645,32 @@ SlotLayout layout_for(int m, int n, long long nnz, bool kind, bool v0, int hist_
   return s;
 }
 
-int copy_in(void* dst, const void* src, size_t bytes, int memory, cudaStream_t st) {
+// The device work of one admit call, gathered so that it takes two launches
+// whatever the number of LPs: the copies of device-resident inputs and the
+// zeroing of the slots' states (pieces of at most 256 KB, one gather_copy
+// launch), and the validation of every LP's arrays (one admission_check).
+struct AdmitBatch {
+  std::vector<CopyPiece> pieces;
+  std::vector<AdmitTasks> tasks;
+  int gx = 1;
+  void add(void* dst, const void* src, size_t bytes) {
+    constexpr size_t kPiece = (size_t)1 << 18;
+    for (size_t o = 0; o < bytes; o += kPiece)
+      pieces.push_back({(char*)dst + o, src ? (const char*)src + o : nullptr,
+                        (long long)std::min(kPiece, bytes - o)});
+  }
+};
+
+// Host inputs are copied at once (DMA from the caller's buffers); device
+// inputs join the admit call's gathered copy.
+int copy_in(AdmitBatch& ab, void* dst, const void* src, size_t bytes, int memory, cudaStream_t st) {
   if (bytes == 0) return PDLP_OK;
   if (!src) return fail(PDLP_ERR_ARG, "a required input array is NULL");
-  PDLP_CUDA(cudaMemcpyAsync(dst, src, bytes,
-                            memory == PDLP_MEM_HOST ? cudaMemcpyHostToDevice
-                                                    : cudaMemcpyDeviceToDevice, st));
+  if (memory == PDLP_MEM_HOST) {
+    PDLP_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+  } else {
+    ab.add(dst, src, bytes);
+  }
   return PDLP_OK;
 }
 
@@ -1028,7 +1092,7 @@ static int admit_args(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_para
 // Phase 1.  pd.P, pd.prm, pd.rp and pd.cp are set by the caller (the pointer
 // arrays already readable on the host).  On success the slot is reserved,
 // the arena taken and the copies and the check enqueued on the stream.
-static int admit_enqueue(pdlp_batch* b, Pending& pd) {
+static int admit_enqueue(pdlp_batch* b, Pending& pd, AdmitBatch& ab) {
   const pdlp_problem_desc* P = pd.P;
   const int m = P->m, n = P->n;
   const long long nnz = P->nnz;
@@ -1107,22 +1171,22 @@ static int admit_enqueue(pdlp_batch* b, Pending& pd) {
   const int mem = P->memory;
   // the state's error word doubles as the validation flag
   int* err_flag = &b->d_state[slot].error;
-  PDLP_CUDA(cudaMemsetAsync(&b->d_state[slot], 0, sizeof(State), st));
+  ab.add(&b->d_state[slot], nullptr, sizeof(State));
   long long* rp64 = (long long*)at(L.tmp64);
   long long* cp64 = rp64 + (m + 1);
-  if ((rc = copy_in(rp64, P->rp, sizeof(int64_t) * (m + 1), mem, st))) return rc;
-  if ((rc = copy_in(cp64, P->cp, sizeof(int64_t) * (n + 1), mem, st))) return rc;
-  if ((rc = copy_in(at(L.ri), P->ri, sizeof(int) * nnz, mem, st))) return rc;
-  if ((rc = copy_in(at(L.ci), P->ci, sizeof(int) * nnz, mem, st))) return rc;
-  if ((rc = copy_in(at(L.rx0), P->rx, sizeof(double) * nnz, mem, st))) return rc;
-  if ((rc = copy_in(at(L.cx0), P->cx, sizeof(double) * nnz, mem, st))) return rc;
-  if ((rc = copy_in(at(L.c0), P->c, sizeof(double) * n, mem, st))) return rc;
-  if ((rc = copy_in(at(L.lo0), P->col_lb, sizeof(double) * n, mem, st))) return rc;
-  if ((rc = copy_in(at(L.hi0), P->col_ub, sizeof(double) * n, mem, st))) return rc;
-  if ((rc = copy_in(at(L.rl0), P->row_lb, sizeof(double) * m, mem, st))) return rc;
-  if ((rc = copy_in(at(L.ru0), P->row_ub, sizeof(double) * m, mem, st))) return rc;
-  if (has_kind && (rc = copy_in(at(L.kind), P->kind, (size_t)n, mem, st))) return rc;
-  if (has_v0 && (rc = copy_in(at(L.v0), prm.power_start, sizeof(double) * n, mem, st))) return rc;
+  if ((rc = copy_in(ab, rp64, P->rp, sizeof(int64_t) * (m + 1), mem, st))) return rc;
+  if ((rc = copy_in(ab, cp64, P->cp, sizeof(int64_t) * (n + 1), mem, st))) return rc;
+  if ((rc = copy_in(ab, at(L.ri), P->ri, sizeof(int) * nnz, mem, st))) return rc;
+  if ((rc = copy_in(ab, at(L.ci), P->ci, sizeof(int) * nnz, mem, st))) return rc;
+  if ((rc = copy_in(ab, at(L.rx0), P->rx, sizeof(double) * nnz, mem, st))) return rc;
+  if ((rc = copy_in(ab, at(L.cx0), P->cx, sizeof(double) * nnz, mem, st))) return rc;
+  if ((rc = copy_in(ab, at(L.c0), P->c, sizeof(double) * n, mem, st))) return rc;
+  if ((rc = copy_in(ab, at(L.lo0), P->col_lb, sizeof(double) * n, mem, st))) return rc;
+  if ((rc = copy_in(ab, at(L.hi0), P->col_ub, sizeof(double) * n, mem, st))) return rc;
+  if ((rc = copy_in(ab, at(L.rl0), P->row_lb, sizeof(double) * m, mem, st))) return rc;
+  if ((rc = copy_in(ab, at(L.ru0), P->row_ub, sizeof(double) * m, mem, st))) return rc;
+  if (has_kind && (rc = copy_in(ab, at(L.kind), P->kind, (size_t)n, mem, st))) return rc;
+  if (has_v0 && (rc = copy_in(ab, at(L.v0), prm.power_start, sizeof(double) * n, mem, st))) return rc;
   AdmitTasks T;
   T.rp64 = rp64; T.rp32 = (int*)at(L.rp32); T.m = m;
   T.cp64 = cp64; T.cp32 = (int*)at(L.cp32); T.n = n;
@@ -1132,10 +1196,57 @@ static int admit_enqueue(pdlp_batch* b, Pending& pd) {
   T.rl0 = (const double*)at(L.rl0); T.ru0 = (const double*)at(L.ru0);
   T.err = err_flag;
   const long long most = std::max<long long>({nnz, (long long)m + 1, (long long)n + 1});
-  const int gx = (int)std::max(1LL, std::min(1024LL, (most + 255) / 256));
-  admission_check<<<dim3(gx, 11), 256, 0, st>>>(T);
-  PDLP_CUDA(cudaGetLastError());
-  count_launches(1);
+  ab.gx = std::max(ab.gx, (int)std::max(1LL, std::min(1024LL, (most + 255) / 256)));
+  ab.tasks.push_back(T);
+  return PDLP_OK;
+}
+
+// Grows a pinned staging array and its device twin to hold `need` elements
+// (the previous contents are not kept; nothing is in flight on them between
+// admit calls, each of which synchronises its stream).
+template <typename E>
+static int ensure_staging(E** h, E** d, size_t* cap, size_t need) {
+  if (need <= *cap && *h && *d) return PDLP_OK;
+  const size_t n = std::max(need, (size_t)64);
+  if (*h) cudaFreeHost(*h);
+  cudaFree(*d);
+  *h = nullptr;
+  *d = nullptr;
+  *cap = 0;
+  PDLP_CUDA(cudaMallocHost((void**)h, sizeof(E) * n));
+  PDLP_CUDA(cudaMalloc((void**)d, sizeof(E) * n));
+  *cap = n;
+  return PDLP_OK;
+}
+
+// Launches the admit call's gathered copies, then its checks.
+static int admit_flush(pdlp_batch* b, AdmitBatch& ab) {
+  cudaStream_t st = b->stream;
+  int rc;
+  if (!ab.pieces.empty()) {
+    const size_t n = ab.pieces.size();
+    if ((rc = ensure_staging(&b->h_pieces, &b->d_pieces, &b->cap_pieces, n))) return rc;
+    std::memcpy(b->h_pieces, ab.pieces.data(), sizeof(CopyPiece) * n);
+    PDLP_CUDA(cudaMemcpyAsync(b->d_pieces, b->h_pieces, sizeof(CopyPiece) * n,
+                              cudaMemcpyHostToDevice, st));
+    const int g = (int)std::min<size_t>(n, (size_t)std::max(1, b->sms) * 8);
+    gather_copy<<<g, 256, 0, st>>>(b->d_pieces, (int)n);
+    PDLP_CUDA(cudaGetLastError());
+    count_launches(1);
+  }
+  if (!ab.tasks.empty()) {
+    const size_t n = ab.tasks.size();
+    if ((rc = ensure_staging(&b->h_tasks, &b->d_tasks, &b->cap_tasks, n))) return rc;
+    std::memcpy(b->h_tasks, ab.tasks.data(), sizeof(AdmitTasks) * n);
+    PDLP_CUDA(cudaMemcpyAsync(b->d_tasks, b->h_tasks, sizeof(AdmitTasks) * n,
+                              cudaMemcpyHostToDevice, st));
+    for (size_t o = 0; o < n; o += 65535) {
+      const unsigned z = (unsigned)std::min<size_t>(65535, n - o);
+      admission_check<<<dim3(ab.gx, 11, z), 256, 0, st>>>(b->d_tasks + o);
+      PDLP_CUDA(cudaGetLastError());
+      count_launches(1);
+    }
+  }
   return PDLP_OK;
 }
 
@@ -1309,25 +1420,36 @@ static int admit_many(pdlp_batch* b, int count, const pdlp_problem_desc* const* 
     }
   }
   if (need) PDLP_CUDA(cudaStreamSynchronize(st));
+  AdmitBatch ab;
   for (int i = 0; i < count; ++i) {
     if (code[i] != PDLP_OK) continue;
-    const int rc = admit_enqueue(b, pd[i]);
+    const size_t np = ab.pieces.size(), nt = ab.tasks.size();
+    const int rc = admit_enqueue(b, pd[i], ab);
     if (rc != PDLP_OK) {
+      ab.pieces.resize(np);             // nothing of a refused LP is copied or checked
+      ab.tasks.resize(nt);
       cudaStreamSynchronize(st);        // its enqueued copies end before the arena is reused
       admit_abandon(b, pd[i]);
       note(i, rc);
     }
   }
-  // every verdict in one read-back
   cudaError_t e = cudaSuccess;
-  for (int i = 0; i < count; ++i) {
-    b->h_errs[i] = 0;
-    if (code[i] == PDLP_OK && e == cudaSuccess)
-      e = cudaMemcpyAsync(&b->h_errs[i], &b->d_state[pd[i].slot].error, sizeof(int),
-                          cudaMemcpyDeviceToHost, st);
+  {
+    const int frc = admit_flush(b, ab);
+    if (frc != PDLP_OK) {
+      cudaStreamSynchronize(st);
+      for (int i = 0; i < count; ++i) if (code[i] == PDLP_OK) admit_abandon(b, pd[i]);
+      return frc;
+    }
   }
+  // every verdict in one read-back (the states of all slots; nothing runs
+  // between steps, so the running slots' copies are current too)
+  e = cudaMemcpyAsync(b->h_state, b->d_state, sizeof(State) * b->slots.size(),
+                      cudaMemcpyDeviceToHost, st);
   const cudaError_t e2 = cudaStreamSynchronize(st);
   if (e == cudaSuccess) e = e2;
+  for (int i = 0; i < count; ++i)
+    b->h_errs[i] = (code[i] == PDLP_OK && e == cudaSuccess) ? b->h_state[pd[i].slot].error : 0;
   if (e != cudaSuccess) {
     for (int i = 0; i < count; ++i) if (code[i] == PDLP_OK) admit_abandon(b, pd[i]);
     return cuda_fail(e, "admission copies");
@@ -1483,6 +1605,10 @@ int pdlp_batch_destroy(pdlp_batch* b) {
   if (b->h_init) cudaFreeHost(b->h_init);
   if (b->h_errs) cudaFreeHost(b->h_errs);
   if (b->h_ptrs) cudaFreeHost(b->h_ptrs);
+  if (b->h_pieces) cudaFreeHost(b->h_pieces);
+  if (b->h_tasks) cudaFreeHost(b->h_tasks);
+  cudaFree(b->d_pieces);
+  cudaFree(b->d_tasks);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   delete b;

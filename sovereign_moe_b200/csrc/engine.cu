@@ -563,6 +563,8 @@ struct pdlp_batch {
   CopyPiece* h_pieces = nullptr;       // pinned / device: an admit call's copy pieces
   CopyPiece* d_pieces = nullptr;
   size_t cap_pieces = 0;
+  char* h_stage = nullptr;             // pinned: a re-plan's tile lists, packed for upload
+  size_t cap_stage = 0;
   AdmitTasks* h_tasks = nullptr;       // pinned / device: an admit call's device checks
   AdmitTasks* d_tasks = nullptr;
   size_t cap_tasks = 0;
@@ -936,22 +938,39 @@ static int rebuild(pdlp_batch* b) {
                             sizeof(double)))) return rc;
   if ((rc = ensure_capacity((void**)&b->d_gcounters, &b->cap_gcounters, groups.size(),
                             sizeof(unsigned)))) return rc;
+  // every list packed into one pinned staging area and uploaded from there:
+  // the copies are asynchronous, and the staging area is next written by the
+  // next re-plan, after the launch that follows this one has been waited for
   cudaStream_t st = b->stream;
-  if (!rt.empty()) PDLP_CUDA(cudaMemcpyAsync(b->d_rtiles, rt.data(), rt.size() * sizeof(Tile), cudaMemcpyHostToDevice, st));
-  if (!ct.empty()) PDLP_CUDA(cudaMemcpyAsync(b->d_ctiles, ct.data(), ct.size() * sizeof(Tile), cudaMemcpyHostToDevice, st));
-  PDLP_CUDA(cudaMemcpyAsync(b->d_rwarp, rwr.data(), rwr.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-  PDLP_CUDA(cudaMemcpyAsync(b->d_cwarp, cwr.data(), cwr.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-  PDLP_CUDA(cudaMemcpyAsync(b->d_teams, teams.data(), teams.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-  if (!groups.empty())
-    PDLP_CUDA(cudaMemcpyAsync(b->d_group_tiles, groups.data(), groups.size() * sizeof(int2),
-                              cudaMemcpyHostToDevice, st));
-  PDLP_CUDA(cudaMemsetAsync(b->d_gcounters, 0, groups.size() * sizeof(unsigned), st));
-  PDLP_CUDA(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2 * b->slots.size(), st));
   std::vector<Inst> insts(b->slots.size());
   for (size_t s = 0; s < b->slots.size(); ++s) insts[s] = b->slots[s].inst;
-  PDLP_CUDA(cudaMemcpyAsync(b->d_inst, insts.data(), insts.size() * sizeof(Inst), cudaMemcpyHostToDevice, st));
-  // the staging vectors die at return: wait for the copies
-  PDLP_CUDA(cudaStreamSynchronize(st));
+  struct Part { void* dst; const void* src; size_t bytes; };
+  const Part parts[] = {
+      {b->d_rtiles, rt.data(), rt.size() * sizeof(Tile)},
+      {b->d_ctiles, ct.data(), ct.size() * sizeof(Tile)},
+      {b->d_rwarp, rwr.data(), rwr.size() * sizeof(int)},
+      {b->d_cwarp, cwr.data(), cwr.size() * sizeof(int)},
+      {b->d_teams, teams.data(), teams.size() * sizeof(int)},
+      {b->d_group_tiles, groups.data(), groups.size() * sizeof(int2)},
+      {b->d_inst, insts.data(), insts.size() * sizeof(Inst)}};
+  size_t total = 0;
+  for (const Part& q : parts) total += (q.bytes + 15) / 16 * 16;
+  if (total > b->cap_stage) {
+    if (b->h_stage) cudaFreeHost(b->h_stage);
+    b->h_stage = nullptr;
+    b->cap_stage = 0;
+    PDLP_CUDA(cudaMallocHost((void**)&b->h_stage, total + total / 2));
+    b->cap_stage = total + total / 2;
+  }
+  size_t off = 0;
+  for (const Part& q : parts) {
+    if (q.bytes == 0) continue;
+    std::memcpy(b->h_stage + off, q.src, q.bytes);
+    PDLP_CUDA(cudaMemcpyAsync(q.dst, b->h_stage + off, q.bytes, cudaMemcpyHostToDevice, st));
+    off += (q.bytes + 15) / 16 * 16;
+  }
+  PDLP_CUDA(cudaMemsetAsync(b->d_gcounters, 0, groups.size() * sizeof(unsigned), st));
+  PDLP_CUDA(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2 * b->slots.size(), st));
   b->dirty = false;
   b->graph_stale = true;
   return PDLP_OK;
@@ -1606,6 +1625,7 @@ int pdlp_batch_destroy(pdlp_batch* b) {
   if (b->h_errs) cudaFreeHost(b->h_errs);
   if (b->h_ptrs) cudaFreeHost(b->h_ptrs);
   if (b->h_pieces) cudaFreeHost(b->h_pieces);
+  if (b->h_stage) cudaFreeHost(b->h_stage);
   if (b->h_tasks) cudaFreeHost(b->h_tasks);
   cudaFree(b->d_pieces);
   cudaFree(b->d_tasks);

@@ -48,8 +48,8 @@ EPS = 1e-6
 # DRAM bytes per algorithmic byte of engine_persistent on this batch, from one
 # ncu capture of the first 256-step launch of
 # `bench.py --workload engine-steps --iters 300`: dram__bytes_read.sum +
-# dram__bytes_write.sum = 80.39 GB against 75.90 GB of algorithmic bytes.
-TRAFFIC_PER_ALGORITHMIC_BYTE = 80.39 / 75.90
+# dram__bytes_write.sum = 80.43 GB against 75.90 GB of algorithmic bytes.
+TRAFFIC_PER_ALGORITHMIC_BYTE = 80.43 / 75.90
 
 
 def load_peaks():

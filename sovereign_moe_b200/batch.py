@@ -21,7 +21,8 @@ import time
 import numpy as np
 
 from . import _lib
-from .pdlp import PDLPParams, _check_device, _to_solution, params_struct, problem_desc
+from .pdlp import (PDLPParams, _check_device, _to_solution, params_struct, problem_desc,
+                   start_with_problem)
 
 __all__ = ["BatchEngine"]
 
@@ -84,6 +85,7 @@ class BatchEngine:
         t0 = time.perf_counter()
         desc, keep = problem_desc(prob)
         p, keep_v0 = params_struct(params, int(prob.A.n), power_start=power_start)
+        keep_v0 = start_with_problem(desc, p, keep_v0)
         if hint:
             p.expected_iterations = float(hint)
         slot = ctypes.c_int32(-1)
@@ -112,6 +114,7 @@ class BatchEngine:
         for i, prob in enumerate(probs):
             d, k = problem_desc(prob)
             p, kv = params_struct(params, int(prob.A.n), power_start=power_start)
+            kv = start_with_problem(d, p, kv)
             if hints is not None:
                 p.expected_iterations = float(hints[i])
             descs[i], prms[i] = d, p

@@ -664,15 +664,24 @@ struct AdmitBatch {
 };
 
 // Host inputs are copied at once (DMA from the caller's buffers); device
-// inputs join the admit call's gathered copy.
+// inputs join the admit call's gathered copy, which a kernel reads: so an
+// array declared as device memory must be device (or managed) memory, and
+// anything else -- a host pointer passed with PDLP_MEM_DEVICE -- is refused
+// here instead of being dereferenced on the device.
 int copy_in(AdmitBatch& ab, void* dst, const void* src, size_t bytes, int memory, cudaStream_t st) {
   if (bytes == 0) return PDLP_OK;
   if (!src) return fail(PDLP_ERR_ARG, "a required input array is NULL");
   if (memory == PDLP_MEM_HOST) {
     PDLP_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
-  } else {
-    ab.add(dst, src, bytes);
+    return PDLP_OK;
   }
+  cudaPointerAttributes attr{};
+  const cudaError_t e = cudaPointerGetAttributes(&attr, src);
+  if (e != cudaSuccess) cudaGetLastError();        // an unknown pointer: not device memory
+  if (e != cudaSuccess || (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged))
+    return fail(PDLP_ERR_ARG, "an input array declared as device memory (PDLP_MEM_DEVICE) is not "
+                              "device memory");
+  ab.add(dst, src, bytes);
   return PDLP_OK;
 }
 

@@ -85,12 +85,60 @@ def _host(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
 
 
+def _on_device(a):
+    """True for a torch tensor in CUDA memory."""
+    return bool(getattr(a, "is_cuda", False))
+
+
+def _numpy(a, dtype=np.float64):
+    """A host view of ``a`` (copied back from the device when it lives there)."""
+    if _on_device(a):
+        return a.detach().to("cpu").numpy().astype(dtype, copy=False)
+    return np.asarray(a, dtype=dtype)
+
+
+def _device_desc(prob):
+    """A ``pdlp_problem_desc`` over CUDA tensors: ``prob``'s arrays stay on the
+    device (converted to the ABI's types there when needed) and the engine
+    copies them into the slot's arena on the device."""
+    import torch
+    A = prob.A
+    f64, i32, i64 = torch.float64, torch.int32, torch.int64
+
+    def dev(a, dt):
+        t = a if torch.is_tensor(a) else torch.as_tensor(np.asarray(a))
+        return t.to(device="cuda", dtype=dt).contiguous()
+
+    arrs = dict(rp=dev(A.rp, i64), ri=dev(A.ri, i32), rx=dev(A.rx, f64),
+                cp=dev(A.cp, i64), ci=dev(A.ci, i32), cx=dev(A.cx, f64),
+                c=dev(prob.c, f64), row_lb=dev(prob.row_lb, f64), row_ub=dev(prob.row_ub, f64),
+                col_lb=dev(prob.col_lb, f64), col_ub=dev(prob.col_ub, f64))
+    kind = getattr(prob, "kind", None)
+    if kind is not None and np.any(_numpy(kind, np.uint8) != 0):
+        arrs["kind"] = dev(kind, torch.uint8)
+    d = _lib.ProblemDesc()
+    d.m, d.n, d.nnz = int(A.m), int(A.n), int(arrs["ci"].numel())
+    for name, a in arrs.items():
+        setattr(d, name, a.data_ptr() if a.numel() else None)
+    for name in ("rp", "cp"):
+        setattr(d, name, arrs[name].data_ptr())
+    d.obj_offset = float(prob.obj_offset)
+    d.sense = -1 if int(prob.sense) == int(ObjSense.MAXIMISE) else 1
+    d.memory = _lib.PDLP_MEM_DEVICE
+    torch.cuda.current_stream().synchronize()    # conversions done before the engine's stream reads
+    return d, arrs
+
+
 def problem_desc(prob, flip_free=True):
-    """A ``pdlp_problem_desc`` over host copies of ``prob``'s arrays.
+    """A ``pdlp_problem_desc`` over ``prob``'s arrays: host copies, or, when
+    the matrix values are a CUDA tensor, the device arrays themselves
+    (``_device_desc``).
 
     Returns ``(desc, keepalive)``; ``keepalive`` must outlive every call that
     uses ``desc``."""
     A = prob.A
+    if _on_device(A.rx):
+        return _device_desc(prob)
     arrs = dict(
         rp=_host(A.rp, np.int64), ri=_host(A.ri, np.int32), rx=_host(A.rx, np.float64),
         cp=_host(A.cp, np.int64), ci=_host(A.ci, np.int32), cx=_host(A.cx, np.float64),
@@ -151,6 +199,19 @@ def params_struct(params: PDLPParams, n: int, time_used: float = 0.0, history_ca
     return p, keep
 
 
+def start_with_problem(desc, p, keep_v0):
+    """The power-iteration start vector lives where the problem does (the C
+    ABI reads it with the problem's memory kind): for a device-resident
+    problem the host vector of ``params_struct`` is copied to the device and
+    ``p.power_start`` points there.  Returns what must be kept alive."""
+    if desc.memory == _lib.PDLP_MEM_DEVICE and keep_v0 is not None and keep_v0.size:
+        import torch
+        keep_v0 = torch.as_tensor(keep_v0, device="cuda")
+        torch.cuda.current_stream().synchronize()
+        p.power_start = keep_v0.data_ptr()
+    return keep_v0
+
+
 def _check_device(device: str):
     if device == "cpu":
         raise ValueError("this PDLP engine runs on the GPU only: use device='gpu' or 'auto'")
@@ -159,7 +220,12 @@ def _check_device(device: str):
 
 
 def solve_pdlp(prob, params: PDLPParams | None = None) -> Solution:
-    """Solve an LP with restarted average PDHG on the GPU."""
+    """Solve an LP with restarted average PDHG on the GPU.
+
+    ``prob`` is the reference's ``Problem`` (or this package's), with NumPy
+    arrays; an object with the same fields whose arrays are torch CUDA
+    tensors (``A.rx`` decides) is solved from device memory, without a copy
+    through the host.  The result is on the host either way."""
     params = params or PDLPParams()
     t0 = time.perf_counter()
     _check_device(params.device)
@@ -169,6 +235,7 @@ def solve_pdlp(prob, params: PDLPParams | None = None) -> Solution:
     desc, keep = problem_desc(prob)
     m, n = int(prob.A.m), int(prob.A.n)
     p, keep_v0 = params_struct(params, n, time_used=time.perf_counter() - t0)
+    keep_v0 = start_with_problem(desc, p, keep_v0)
     x = np.empty(n)
     y = np.empty(m)
     d = np.empty(n)
@@ -213,7 +280,7 @@ def _result_types(prob, params):
 def _to_solution(prob, params, res, x, y, d, hist, elapsed):
     Sol, St, Info = _result_types(prob, params)
     status = St(int(res.status))
-    obj = float(np.asarray(prob.c, dtype=np.float64) @ x) + float(prob.obj_offset)
+    obj = float(_numpy(prob.c) @ x) + float(prob.obj_offset)
     h = hist[:5 * int(res.history_len)].reshape(-1, 5)
     history = [(int(r[0]), float(r[1]), float(r[2]), float(r[3]), float(r[4])) for r in h]
     info = Info(iterations=int(res.iterations), restarts=int(res.restarts),

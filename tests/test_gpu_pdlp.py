@@ -281,3 +281,28 @@ def test_sizes_beyond_int32_entries_are_refused(require_gpu):
         code = eng.lib.pdlp_batch_admit(eng.h, ctypes.byref(d), ctypes.byref(p), ctypes.byref(slot))
         assert code == _lib.PDLP_ERR_ARG
         assert "int32" in eng.lib.pdlp_last_error().decode()
+
+
+def test_device_resident_problem_equals_host(require_gpu):
+    """An LP whose arrays are torch CUDA tensors is solved from device memory
+    (descriptor memory = device) to the same bits as the NumPy LP."""
+    import torch
+    from types import SimpleNamespace
+    from sovereign_moe_b200.pdlp import PDLPParams, problem_desc, solve_pdlp
+    from sovereign_moe_b200.workloads import uneven_batch
+    from sovereign_moe_b200 import _lib
+    prob = uneven_batch(seed=41, count=1, m_lo=300, m_hi=900)[0].problem
+    dev = lambda a: torch.as_tensor(np.asarray(a), device="cuda")  # noqa: E731
+    A = prob.A
+    dprob = SimpleNamespace(
+        A=SimpleNamespace(m=A.m, n=A.n, rp=dev(A.rp), ri=dev(A.ri), rx=dev(A.rx),
+                          cp=dev(A.cp), ci=dev(A.ci), cx=dev(A.cx)),
+        c=dev(prob.c), row_lb=dev(prob.row_lb), row_ub=dev(prob.row_ub),
+        col_lb=dev(prob.col_lb), col_ub=dev(prob.col_ub), obj_offset=prob.obj_offset,
+        sense=prob.sense, kind=None)
+    assert problem_desc(dprob)[0].memory == _lib.PDLP_MEM_DEVICE
+    p = PDLPParams(device="gpu", eps_abs=1e-6, eps_rel=1e-6)
+    a, b = solve_pdlp(prob, p), solve_pdlp(dprob, p)
+    assert a.status == b.status and a.iterations == b.iterations
+    assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y)
+    assert a.objective == b.objective

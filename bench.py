@@ -688,7 +688,10 @@ def run_spmv(args):
     CUDA events after an L2 flush: a 256 MB write followed by a 256 MB read,
     so that the cache holds no dirty lines whose write-back would land in the
     timed call.  Every variant of the row-block pass is timed, then the
-    autotuner's choice (``pdlp_spmv_tune_*``) on the same matrix."""
+    autotuner's choice (``pdlp_spmv_tune_*``) on the same matrix.  The planned
+    kernel (``pdlp_spmv_plan_*``) is timed the same way, and also as a stream
+    of 30 products over copies of the matrix (at least twice L2 together)
+    between one pair of events ("planned_stream", per product)."""
     import ctypes
     import torch
     from sovereign_moe_b200 import _lib
@@ -774,8 +777,42 @@ def run_spmv(args):
                     return statistics.median(times)
 
                 per["planned"] = timed_plan()
-                _lib.check(lib.pdlp_spmv_plan_status(plan, stream.cuda_stream))
-                lib.pdlp_spmv_plan_destroy(plan)
+
+                # a stream of products, as PDHG makes them: copies of the
+                # matrix (indices and values, each with its own plan; together
+                # at least twice the 126 MB L2) in turn, 30 products between
+                # one pair of events, so each product reads its matrix from
+                # HBM and the per-call launch floor is paid once
+                ncopies = max(3, -(-260_000_000 // algo))
+                copies = [(rp, ri, rx, plan)]
+                for _ in range(ncopies - 1):
+                    rp2, ri2, rx2 = rp.clone(), ri.clone(), rx.clone()
+                    pl2 = ctypes.c_void_p()
+                    _lib.check(lib.pdlp_spmv_plan_create(int(r), int(c), rp2.data_ptr(),
+                                                         ri2.data_ptr(), stream.cuda_stream,
+                                                         ctypes.byref(pl2)))
+                    copies.append((rp2, ri2, rx2, pl2))
+                for q in range(2 * ncopies):
+                    _, _, rxq, plq = copies[q % ncopies]
+                    _lib.check(prun(plq, rxq.data_ptr(), x.data_ptr(), y.data_ptr(),
+                                    stream.cuda_stream))
+                stream_ms = []
+                for _ in range(max(3, args.steps)):
+                    flush_l2()
+                    e0, e1 = _sync_events(torch)
+                    e0.record()
+                    for q in range(30):
+                        _, _, rxq, plq = copies[q % ncopies]
+                        _lib.check(prun(plq, rxq.data_ptr(), x.data_ptr(), y.data_ptr(),
+                                        stream.cuda_stream))
+                    e1.record()
+                    e1.synchronize()
+                    stream_ms.append(e0.elapsed_time(e1) / 30)
+                per["planned_stream"] = statistics.median(stream_ms)
+                for _, _, _, plq in copies:
+                    _lib.check(lib.pdlp_spmv_plan_status(plq, stream.cuda_stream))
+                    lib.pdlp_spmv_plan_destroy(plq)
+                del copies
                 best = ctypes.c_int32(0)
                 tms = (ctypes.c_double * 3)()
                 _lib.check(tune(int(r), rp.data_ptr(), ri.data_ptr(), rx.data_ptr(), x.data_ptr(),
@@ -791,6 +828,10 @@ def run_spmv(args):
                              "frac_of_measured_hbm": algo / ms / 1e6 / peak,
                              "planned": {"ms": pms, "GBps": algo / pms / 1e6,
                                          "frac_of_measured_hbm": algo / pms / 1e6 / peak,
+                                         "stream_ms": per["planned_stream"],
+                                         "stream_copies": ncopies,
+                                         "stream_frac_of_measured_hbm":
+                                             algo / per["planned_stream"] / 1e6 / peak,
                                          "plan_seconds": pinfo.seconds, "tiles": pinfo.tiles,
                                          "banded_tiles": pinfo.banded_tiles,
                                          "entries_in_band": pinfo.entries_in_band,

@@ -65,6 +65,7 @@ struct pdlp_spmv_plan {
   int* cta_first = nullptr;     // [nctas + 1], device
   int* long_rows = nullptr;     // row (within its tile) of each row of 65..2048 entries
   int* halo_cols = nullptr;     // columns of each tile's halo, in tile order
+  uint16_t* perm = nullptr;     // per row: the order in which a tile's short rows meet lanes
   int* status = nullptr;        // device word: 0 or the error of a wait that ran out
   int64_t base = 0;             // the caller's rp[0]: entry q of the plan is the caller's base + q
   int ntiles = 0, nctas = 0;
@@ -107,8 +108,10 @@ struct PlanTile {
   int nhalo;       // halo columns, listed from halo_first in halo_cols
   int halo_first;
   int staged;      // 1: every entry's x is staged (no gather from global memory)
+  int nshort;      // rows of at most kLaneRow entries: perm[r0 .. r0 + nshort)
+  int pad;
 };
-static_assert(sizeof(PlanTile) == 56, "PlanTile layout");
+static_assert(sizeof(PlanTile) == 64, "PlanTile layout");
 
 // Byte layout of one stage.  Each copied array has room for the copy's start
 // being rounded down to a 16-byte chunk; every size is a multiple of 16, so
@@ -119,7 +122,9 @@ template <typename T>
 struct StageLayout {
   static constexpr int kPer = 16 / (int)sizeof(T);
   static constexpr int desc_bytes = 64;                         // the tile's PlanTile
-  static constexpr int rp_off = desc_bytes;
+  static constexpr int perm_off = desc_bytes;
+  static constexpr int perm_bytes = (kPlanRows + 8) * 2;
+  static constexpr int rp_off = perm_off + perm_bytes;
   static constexpr int rp_bytes = (kPlanRows + 2) * 8;
   static constexpr int idx_off = rp_off + rp_bytes;
   static constexpr int idx_bytes = (kPlanNnz + 4) * 4;
@@ -206,19 +211,19 @@ __device__ __forceinline__ void consume_tile(const PlanTile& t, const unsigned c
   const T* sval =
       reinterpret_cast<const T*>(st + L::val_off) + (int)((base + t.p0) & (L::kPer - 1));
   const T* sx = reinterpret_cast<const T*>(st + L::x_off) + (t.blo & (L::kPer - 1));
+  const uint16_t* sperm = reinterpret_cast<const uint16_t*>(st + L::perm_off) + (t.r0 & 7);
   // a rewritten index: staged x (window or halo), or -(column + 1)
   auto xval = [&](int jj) -> T {
     if (STAGED) return sx[jj];
     return jj >= 0 ? sx[jj] : __ldg(x + (-1 - jj));
   };
-  for (int rb = gw * 32; rb < t.nr; rb += kGroupW * 32) {
-    const int li = rb + lane;
-    int ps = 0, pe = 0;
-    if (li < t.nr) {
-      ps = (int)(srp[li] - t.p0);
-      pe = (int)(srp[li + 1] - t.p0);
-    }
-    if (li < t.nr && pe - ps <= kLaneRow) {
+  // the short rows, one per lane, in the plan's order: the 32 rows of a warp
+  // start at different banks, so the lanes' loads of indices and values do
+  // not collide in shared memory
+  for (int rb = gw * 32; rb < t.nshort; rb += kGroupW * 32) {
+    if (rb + lane < t.nshort) {
+      const int li = sperm[rb + lane];
+      const int ps = (int)(srp[li] - t.p0), pe = (int)(srp[li + 1] - t.p0);
       T a = T(0);
       int q = ps;
       for (; q + 8 <= pe; q += 8) {         // eight entries' loads in flight
@@ -277,7 +282,8 @@ __global__ void __launch_bounds__(kPlanThreads, 1) spmv_plan_kernel(
     const PlanTile* __restrict__ tiles, const int* __restrict__ cta_first,
     const int64_t* __restrict__ rp, const int* __restrict__ idx, const T* __restrict__ rx,
     const T* __restrict__ x, T* __restrict__ y, const int* __restrict__ long_rows,
-    const int* __restrict__ halo_cols, long long base, int* status) {
+    const int* __restrict__ halo_cols, const uint16_t* __restrict__ perm, long long base,
+    int* status) {
   using L = StageLayout<T>;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ unsigned long long full[kPlanStages], empty[kPlanStages];
@@ -324,11 +330,13 @@ __global__ void __launch_bounds__(kPlanThreads, 1) spmv_plan_kernel(
           if (t.kind == TILE_HUGE) {              // read from global memory by a consumer warp
             mbar_arrive(&full[s]);
           } else {
+            const unsigned bperm = lbulk_bytes<2>(t.r0, t.nshort);
             const unsigned brp = lbulk_bytes<8>(t.r0, t.nr + 1);
             const unsigned bidx = lbulk_bytes<4>(t.p0, t.cnt);
             const unsigned bval = lbulk_bytes<(int)sizeof(T)>(base + t.p0, t.cnt);
             const unsigned bx = lbulk_bytes<(int)sizeof(T)>(t.blo, t.bcnt);
-            mbar_arrive_tx(&full[s], brp + bidx + bval + bx);
+            mbar_arrive_tx(&full[s], bperm + brp + bidx + bval + bx);
+            lbulk_stage<2>(st + L::perm_off, perm, t.r0, bperm, &full[s]);
             lbulk_stage<8>(st + L::rp_off, rp, t.r0, brp, &full[s]);
             lbulk_stage<4>(st + L::idx_off, idx, t.p0, bidx, &full[s]);
             lbulk_stage<(int)sizeof(T)>(st + L::val_off, rx, base + t.p0, bval, &full[s]);
@@ -511,6 +519,7 @@ void free_plan(pdlp_spmv_plan* p) {
   cudaFree(p->cta_first);
   cudaFree(p->long_rows);
   cudaFree(p->halo_cols);
+  cudaFree(p->perm);
   cudaFree(p->status);
   delete p;
 }
@@ -563,6 +572,8 @@ int plan_create(int32_t m, int32_t n, const int64_t* rp, const int32_t* ri, cuda
   std::vector<int> longs, halos, halo, scratch;
   std::vector<std::pair<int, int>> pairs;
   std::vector<int32_t> pidx((size_t)nnz);
+  std::vector<uint16_t> hperm((size_t)m + 8, 0);
+  std::vector<std::pair<int, int>> order;
   pdlp_spmv_plan_info info{};
   for (int i = 0; i < m;) {
     const long long len = hrp[i + 1] - hrp[i];
@@ -595,6 +606,25 @@ int plan_create(int32_t m, int32_t n, const int64_t* rp, const int32_t* ri, cuda
       }
     }
     t.nlong = (int)longs.size() - t.long_first;
+    // the short rows' order for the lanes: bucketed by the bank their first
+    // index lands on in the stage ((p0 + row start) mod 32, p0 counted from
+    // the 16-byte boundary the copy starts at), then taken one per bucket in
+    // turn, so that each 32 consecutive rows start on different banks
+    {
+      order.clear();
+      int rank[32] = {0};
+      for (int r = start; r < i; ++r) {
+        if (hrp[r + 1] - hrp[r] > kLaneRow) continue;
+        const int bank = (int)(((hrp[start] & 3) + (hrp[r] - hrp[start])) & 31);
+        order.push_back({rank[bank]++ * 32 + bank, r - start});
+      }
+      std::stable_sort(order.begin(), order.end(),
+                       [](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+                         return a.first < b.first;
+                       });
+      t.nshort = (int)order.size();
+      for (int k = 0; k < t.nshort; ++k) hperm[(size_t)start + k] = (uint16_t)order[k].second;
+    }
     const int* tri = hri.data() + hrp[start];
     choose_window(tri, cnt, &t.blo, &t.bcnt, scratch);
     const long long staged =
@@ -652,6 +682,7 @@ int plan_create(int32_t m, int32_t n, const int64_t* rp, const int32_t* ri, cuda
   if (e == cudaSuccess) e = upload(&p->cta_first, first.data(), first.size(), st);
   if (e == cudaSuccess) e = upload(&p->long_rows, longs.data(), longs.size(), st);
   if (e == cudaSuccess) e = upload(&p->halo_cols, halos.data(), halos.size(), st);
+  if (e == cudaSuccess) e = upload(&p->perm, hperm.data(), hperm.size(), st);
   if (e == cudaSuccess) e = cudaMalloc((void**)&p->status, sizeof(int));
   if (e == cudaSuccess) e = cudaMemsetAsync(p->status, 0, sizeof(int), st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);   // the host vectors go out of scope
@@ -695,7 +726,7 @@ int plan_run(pdlp_spmv_plan* p, const T* rx, const T* x, T* y, cudaStream_t st) 
     return fail(PDLP_ERR_ARG, "rx and x must be 16-byte aligned (bulk copies)");
   spmv_plan_kernel<T><<<p->nctas, kPlanThreads, kPlanStages * StageLayout<T>::bytes, st>>>(
       static_cast<const PlanTile*>(p->tiles), p->cta_first, p->rp, p->idx, rx, x, y,
-      p->long_rows, p->halo_cols, p->base, p->status);
+      p->long_rows, p->halo_cols, p->perm, p->base, p->status);
   count_launches(1);
   PDLP_CUDA(cudaGetLastError());
   return PDLP_OK;

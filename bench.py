@@ -523,6 +523,10 @@ def run_gpu(args, rank, world):
                "sample": f"{solved} of the {N_LP} LPs, spread over the size range "
                          f"(bit-reversed nnz rank), solved by the CPU restatement in {dt:.1f} s"}
 
+    served = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        served = serving_sample()
+
     if rank == 0:
         total_nnz = sum(k.problem.A.nnz for k in lps)
         line = {
@@ -566,6 +570,7 @@ def run_gpu(args, rank, world):
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": int(launches),
+            "serving": served,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -1029,6 +1034,32 @@ def run_precision(args):
     return 0
 
 
+def serving_sample(count=96, rate=1000.0, max_rows=2000, slots=128):
+    """Config 5's small class (rows up to 2,000: 70% of the mixture) as a
+    Poisson stream of ``count`` requests at ``rate`` per second, served with
+    continuous batching (``serving.Server``) and, on the same GPU, one
+    ``solve_pdlp`` at a time in arrival order (the reference server's
+    discipline); every objective is checked against its known optimum."""
+    from sovereign_moe_b200.serving import Server, latency_summary, serve_one_at_a_time
+    from sovereign_moe_b200.workloads import serving_stream
+    stream = serving_stream(seed=0, count=count, rate=rate, max_rows=max_rows)
+    items = [(t, k.problem) for t, k in stream]
+    with Server(max_slots=slots) as srv:
+        done, st = srv.serve(items)
+    one, st1 = serve_one_at_a_time(items)
+    wrong = sum(1 for r, (t, k) in zip(done, stream)
+                if abs(r.solution.objective - k.f_star) / max(1.0, abs(k.f_star)) > 1e-6)
+    return {"value": st.solves_per_s, "unit": "solves/s",
+            "latency_s": latency_summary(st.latencies),
+            "one_at_a_time": {"value": st1.solves_per_s, "unit": "solves/s",
+                              "latency_s": latency_summary(st1.latencies)},
+            "speedup_vs_one_at_a_time": st.solves_per_s / max(st1.solves_per_s, 1e-12),
+            "max_concurrent": st.max_concurrent, "objectives_off_by_over_1e-6": wrong,
+            "config": {"workload": "poisson_small_class", "count": count, "rate_per_s": rate,
+                       "max_rows": max_rows, "slots": slots,
+                       "timing": "wall clock, host server loop included in both arms"}}
+
+
 def run_serving(args):
     """Poisson arrivals served with continuous batching vs one at a time."""
     from sovereign_moe_b200.serving import Server, latency_summary, serve_one_at_a_time
@@ -1062,6 +1093,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--dump-lps", default=None,
                     help="write each LP's size, iterations and device start/end (JSON)")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="skip the served-stream sample after the timed steps")
     ap.add_argument("--no-public", action="store_true",
                     help="skip the one-at-a-time pass through the public solve_pdlp")
     ap.add_argument("--workload", default="batch",

@@ -17,7 +17,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def test_headline_line_has_every_contract_key(require_gpu):
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--steps", "1",
-                          "--warmup", "3", "--no-cpu", "--no-public"], capture_output=True,
+                          "--warmup", "3", "--no-cpu", "--no-public",
+                          "--no-serving"], capture_output=True,
                          text=True,
                          cwd=ROOT, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]

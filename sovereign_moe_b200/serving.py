@@ -87,6 +87,9 @@ class Server:
         self.engine = BatchEngine(max_slots=max_slots, memory_budget=memory_budget, **engine_kw)
         self.max_slots = int(max_slots)
         self.chunk_steps = int(chunk_steps)
+        # chunks this many times longer once every request has arrived and
+        # none is queued (nothing to admit between chunks)
+        self.idle_chunks = 4
         self.queue: deque = deque()
         self.inflight: dict = {}
         # iteration estimates learned from the requests served so far: the
@@ -155,7 +158,10 @@ class Server:
                 self.queue.append(pending.popleft())
             self._admit_from_queue(now, stats)
             if self.inflight:
-                self.engine.step(self.chunk_steps)
+                # with nothing left to admit, longer chunks: fewer host round
+                # trips (each chunk ends in a synchronisation and a re-plan)
+                idle = not pending and not self.queue
+                self.engine.step(self.chunk_steps * (self.idle_chunks if idle else 1))
                 stats.chunks += 1
                 self._harvest(now, stats, done)
             elif pending:

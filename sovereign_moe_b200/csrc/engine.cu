@@ -686,8 +686,7 @@ int copy_in(AdmitBatch& ab, void* dst, const void* src, size_t bytes, int memory
 }
 
 // Contiguous chunks of the tile list with about equal work, one per block.
-void block_ranges(const std::vector<double>& w, int G, std::vector<int>& out) {
-  const size_t T = w.size();
+void block_ranges(const double* w, size_t T, int G, std::vector<int>& out) {
   double total = 0.0;
   for (size_t i = 0; i < T; ++i) total += w[i];
   out.assign(G + 1, (int)T);
@@ -706,16 +705,6 @@ void block_ranges(const std::vector<double>& w, int G, std::vector<int>& out) {
 
 // Group the tiles of one instance-side into reduction groups of kGroupTiles
 // consecutive tiles; appends (tile range) per group and stamps each tile.
-static void make_groups(std::vector<Tile>& tiles, int t0, int t1, int group_base,
-                        std::vector<int2>& groups) {
-  for (int g0 = t0; g0 < t1; g0 += kGroupTiles) {
-    const int g1 = std::min(t1, g0 + kGroupTiles);
-    const int gid = group_base + (int)groups.size();
-    for (int t = g0; t < g1; ++t) tiles[t].group = gid;
-    groups.push_back(make_int2(g0, g1));
-  }
-}
-
 // Iterations an instance is expected to need still, or a negative value when
 // nothing is known.  From its own progress once its checks span at least
 // kRateSpan iterations: the largest residual-to-tolerance ratio of the
@@ -839,60 +828,58 @@ static std::vector<int> plan_teams(const pdlp_batch* b, const std::vector<int>& 
 }
 
 static int rebuild(pdlp_batch* b) {
-  std::vector<Tile> rt, ct;
-  std::vector<double> rw, cw;
-  for (size_t s = 0; s < b->slots.size(); ++s) {
-    Slot& sl = b->slots[s];
-    if (!sl.used || !sl.running) continue;
-    sl.inst.rt_begin = (int)rt.size();
-    rt.insert(rt.end(), sl.rt.begin(), sl.rt.end());
-    rw.insert(rw.end(), sl.rtw.begin(), sl.rtw.end());
-    sl.inst.rt_end = (int)rt.size();
-    sl.inst.ct_begin = (int)ct.size();
-    ct.insert(ct.end(), sl.ct.begin(), sl.ct.end());
-    cw.insert(cw.end(), sl.ctw.begin(), sl.ctw.end());
-    sl.inst.ct_end = (int)ct.size();
-  }
-  // reduction groups: row-side groups first, then column-side groups
-  std::vector<int2> rgroups, cgroups;
-  for (size_t s = 0; s < b->slots.size(); ++s) {
-    Slot& sl = b->slots[s];
-    if (!sl.used || !sl.running) continue;
-    sl.inst.rg_begin = (int)rgroups.size();
-    make_groups(rt, sl.inst.rt_begin, sl.inst.rt_end, 0, rgroups);
-    sl.inst.rg_end = (int)rgroups.size();
-  }
-  const int nrg = (int)rgroups.size();
-  for (size_t s = 0; s < b->slots.size(); ++s) {
-    Slot& sl = b->slots[s];
-    if (!sl.used || !sl.running) continue;
-    sl.inst.cg_begin = nrg + (int)cgroups.size();
-    make_groups(ct, sl.inst.ct_begin, sl.inst.ct_end, nrg, cgroups);
-    sl.inst.cg_end = nrg + (int)cgroups.size();
-  }
-  std::vector<int2> groups(rgroups);
-  groups.insert(groups.end(), cgroups.begin(), cgroups.end());
-  b->n_rgroups = nrg;
-  b->n_groups = (int)groups.size();
-  b->n_rtiles = (int)rt.size();
-  b->n_ctiles = (int)ct.size();
-  // persistent grid: enough warps for the larger tile list, at most what is
-  // co-resident, in one team or in one team per instance (plan_teams)
-  const int max_blocks = std::max(1, b->sms * b->coop_blocks_per_sm);
+  // where every running slot's tiles and reduction groups go in the launch's
+  // lists: row-side groups first, then column-side groups (64 consecutive
+  // tiles of a slot per group)
   std::vector<int> run;                       // running slots, in tile order
   for (size_t s = 0; s < b->slots.size(); ++s)
     if (b->slots[s].used && b->slots[s].running) run.push_back((int)s);
+  auto ngroups = [](size_t tiles) { return (int)((tiles + kGroupTiles - 1) / kGroupTiles); };
+  int nrt = 0, nct = 0, nrg = 0, ncg = 0;
+  for (int s : run) {
+    Slot& sl = b->slots[s];
+    sl.inst.rt_begin = nrt;
+    nrt += (int)sl.rt.size();
+    sl.inst.rt_end = nrt;
+    sl.inst.ct_begin = nct;
+    nct += (int)sl.ct.size();
+    sl.inst.ct_end = nct;
+    sl.inst.rg_begin = nrg;
+    nrg += ngroups(sl.rt.size());
+    sl.inst.rg_end = nrg;
+  }
+  for (int s : run) {
+    Slot& sl = b->slots[s];
+    sl.inst.cg_begin = nrg + ncg;
+    ncg += ngroups(sl.ct.size());
+    sl.inst.cg_end = nrg + ncg;
+  }
+  b->n_rgroups = nrg;
+  b->n_groups = nrg + ncg;
+  b->n_rtiles = nrt;
+  b->n_ctiles = nct;
+  // persistent grid: enough warps for the larger tile list, at most what is
+  // co-resident, in one team or in one team per instance (plan_teams)
+  const int max_blocks = std::max(1, b->sms * b->coop_blocks_per_sm);
   const std::vector<int> tblocks = plan_teams(b, run, max_blocks);
   // per warp tile ranges, then the team arrays: block_team[G], team_blocks[T],
   // team_first[T]
   std::vector<int> rwr, cwr, teams;
   if (tblocks.empty()) {
+    std::vector<double> rw, cw;                 // one team splits every running tile
+    rw.reserve(nrt);
+    cw.reserve(nct);
+    for (int s : run) {
+      const Slot& sl = b->slots[s];
+      rw.insert(rw.end(), sl.rtw.begin(), sl.rtw.end());
+      cw.insert(cw.end(), sl.ctw.begin(), sl.ctw.end());
+    }
     const int want = (std::max(b->n_rtiles, b->n_ctiles) + kWarps - 1) / kWarps;
     int G = std::max(1, std::min(max_blocks, want));
     if (b->force_blocks > 0) G = std::min(G, b->force_blocks);
     b->grid = G;
-    block_ranges(rw, G * kWarps, rwr);
-    block_ranges(cw, G * kWarps, cwr);
+    block_ranges(rw.data(), rw.size(), G * kWarps, rwr);
+    block_ranges(cw.data(), cw.size(), G * kWarps, cwr);
     b->n_teams = 1;
     b->withhold_candidate = G >= 2 ? G - 1 : -1;
     teams.assign(G, 0);
@@ -908,6 +895,7 @@ static int rebuild(pdlp_batch* b) {
     b->n_teams = T;
     b->withhold_candidate = -1;
     std::vector<int> first(T);
+    std::vector<int> pr, pc;
     int fb = 0;
     for (int k = 0; k < T; ++k) {
       Slot& sl = b->slots[run[k]];
@@ -917,12 +905,9 @@ static int rebuild(pdlp_batch* b) {
       if (b->withhold_candidate < 0 && tblocks[k] >= 2) b->withhold_candidate = fb - 1;
       for (int q = 0; q < tblocks[k]; ++q) teams.push_back(k);
       // the team's warps split its own tiles, as one team splits all of them
-      const int r0 = sl.inst.rt_begin, r1 = sl.inst.rt_end;
-      const int c0 = sl.inst.ct_begin, c1 = sl.inst.ct_end;
-      std::vector<double> wr(rw.begin() + r0, rw.begin() + r1), wc(cw.begin() + c0, cw.begin() + c1);
-      std::vector<int> pr, pc;
-      block_ranges(wr, tblocks[k] * kWarps, pr);
-      block_ranges(wc, tblocks[k] * kWarps, pc);
+      const int r0 = sl.inst.rt_begin, c0 = sl.inst.ct_begin;
+      block_ranges(sl.rtw.data(), sl.rtw.size(), tblocks[k] * kWarps, pr);
+      block_ranges(sl.ctw.data(), sl.ctw.size(), tblocks[k] * kWarps, pc);
       for (int q = 0; q < tblocks[k] * kWarps; ++q) {
         rwr.push_back(r0 + pr[q]);
         cwr.push_back(c0 + pc[q]);
@@ -934,36 +919,31 @@ static int rebuild(pdlp_batch* b) {
     for (int k = 0; k < T; ++k) teams.push_back(first[k]);
     b->team_running.assign(T, 1);
   }
+  const size_t ngr = (size_t)b->n_groups;
   int rc;
-  if ((rc = ensure_capacity((void**)&b->d_rtiles, &b->cap_rtiles, rt.size(), sizeof(Tile)))) return rc;
-  if ((rc = ensure_capacity((void**)&b->d_ctiles, &b->cap_ctiles, ct.size(), sizeof(Tile)))) return rc;
+  if ((rc = ensure_capacity((void**)&b->d_rtiles, &b->cap_rtiles, nrt, sizeof(Tile)))) return rc;
+  if ((rc = ensure_capacity((void**)&b->d_ctiles, &b->cap_ctiles, nct, sizeof(Tile)))) return rc;
   if ((rc = ensure_capacity((void**)&b->d_rwarp, &b->cap_rwarp, rwr.size(), sizeof(int)))) return rc;
   if ((rc = ensure_capacity((void**)&b->d_cwarp, &b->cap_cwarp, cwr.size(), sizeof(int)))) return rc;
   if ((rc = ensure_capacity((void**)&b->d_teams, &b->cap_teams, teams.size(), sizeof(int)))) return rc;
   if ((rc = ensure_capacity((void**)&b->d_partials, &b->cap_partials,
-                            (rt.size() + ct.size()) * kNP, sizeof(double)))) return rc;
-  if ((rc = ensure_capacity((void**)&b->d_group_tiles, &b->cap_groups, groups.size(), sizeof(int2)))) return rc;
-  if ((rc = ensure_capacity((void**)&b->d_gpartials, &b->cap_gpartials, groups.size() * kNP,
+                            ((size_t)nrt + nct) * kNP, sizeof(double)))) return rc;
+  if ((rc = ensure_capacity((void**)&b->d_group_tiles, &b->cap_groups, ngr, sizeof(int2)))) return rc;
+  if ((rc = ensure_capacity((void**)&b->d_gpartials, &b->cap_gpartials, ngr * kNP,
                             sizeof(double)))) return rc;
-  if ((rc = ensure_capacity((void**)&b->d_gcounters, &b->cap_gcounters, groups.size(),
+  if ((rc = ensure_capacity((void**)&b->d_gcounters, &b->cap_gcounters, ngr,
                             sizeof(unsigned)))) return rc;
-  // every list packed into one pinned staging area and uploaded from there:
-  // the copies are asynchronous, and the staging area is next written by the
-  // next re-plan, after the launch that follows this one has been waited for
+  // every list is written straight into one pinned staging area and uploaded
+  // from there: the copies are asynchronous, and the staging area is next
+  // written by the next re-plan, after the launch that follows this one has
+  // been waited for
   cudaStream_t st = b->stream;
-  std::vector<Inst> insts(b->slots.size());
-  for (size_t s = 0; s < b->slots.size(); ++s) insts[s] = b->slots[s].inst;
-  struct Part { void* dst; const void* src; size_t bytes; };
-  const Part parts[] = {
-      {b->d_rtiles, rt.data(), rt.size() * sizeof(Tile)},
-      {b->d_ctiles, ct.data(), ct.size() * sizeof(Tile)},
-      {b->d_rwarp, rwr.data(), rwr.size() * sizeof(int)},
-      {b->d_cwarp, cwr.data(), cwr.size() * sizeof(int)},
-      {b->d_teams, teams.data(), teams.size() * sizeof(int)},
-      {b->d_group_tiles, groups.data(), groups.size() * sizeof(int2)},
-      {b->d_inst, insts.data(), insts.size() * sizeof(Inst)}};
-  size_t total = 0;
-  for (const Part& q : parts) total += (q.bytes + 15) / 16 * 16;
+  auto up16 = [](size_t v) { return (v + 15) / 16 * 16; };
+  const size_t b_rt = sizeof(Tile) * (size_t)nrt, b_ct = sizeof(Tile) * (size_t)nct;
+  const size_t b_gr = sizeof(int2) * ngr, b_in = sizeof(Inst) * b->slots.size();
+  const size_t total = up16(b_rt) + up16(b_ct) + up16(b_gr) + up16(b_in) +
+                       up16(rwr.size() * sizeof(int)) + up16(cwr.size() * sizeof(int)) +
+                       up16(teams.size() * sizeof(int));
   if (total > b->cap_stage) {
     if (b->h_stage) cudaFreeHost(b->h_stage);
     b->h_stage = nullptr;
@@ -971,14 +951,48 @@ static int rebuild(pdlp_batch* b) {
     PDLP_CUDA(cudaMallocHost((void**)&b->h_stage, total + total / 2));
     b->cap_stage = total + total / 2;
   }
-  size_t off = 0;
-  for (const Part& q : parts) {
-    if (q.bytes == 0) continue;
+  Tile* srt = reinterpret_cast<Tile*>(b->h_stage);
+  Tile* sct = reinterpret_cast<Tile*>(b->h_stage + up16(b_rt));
+  int2* sgr = reinterpret_cast<int2*>(b->h_stage + up16(b_rt) + up16(b_ct));
+  Inst* sin = reinterpret_cast<Inst*>(b->h_stage + up16(b_rt) + up16(b_ct) + up16(b_gr));
+  for (int s : run) {
+    const Slot& sl = b->slots[s];
+    const Inst& I = sl.inst;
+    for (size_t k = 0; k < sl.rt.size(); ++k) {
+      Tile t = sl.rt[k];
+      t.group = I.rg_begin + (int)(k / kGroupTiles);
+      srt[I.rt_begin + k] = t;
+    }
+    for (int g = I.rg_begin; g < I.rg_end; ++g) {
+      const int g0 = I.rt_begin + (g - I.rg_begin) * kGroupTiles;
+      sgr[g] = make_int2(g0, std::min(I.rt_end, g0 + kGroupTiles));
+    }
+    for (size_t k = 0; k < sl.ct.size(); ++k) {
+      Tile t = sl.ct[k];
+      t.group = I.cg_begin + (int)(k / kGroupTiles);
+      sct[I.ct_begin + k] = t;
+    }
+    for (int g = I.cg_begin; g < I.cg_end; ++g) {
+      const int g0 = I.ct_begin + (g - I.cg_begin) * kGroupTiles;
+      sgr[g] = make_int2(g0, std::min(I.ct_end, g0 + kGroupTiles));
+    }
+  }
+  for (size_t s = 0; s < b->slots.size(); ++s) sin[s] = b->slots[s].inst;
+  size_t off = up16(b_rt) + up16(b_ct) + up16(b_gr) + up16(b_in);
+  struct Part { void* dst; const void* src; size_t bytes; };
+  const Part small[] = {{b->d_rwarp, rwr.data(), rwr.size() * sizeof(int)},
+                        {b->d_cwarp, cwr.data(), cwr.size() * sizeof(int)},
+                        {b->d_teams, teams.data(), teams.size() * sizeof(int)}};
+  for (const Part& q : small) {
     std::memcpy(b->h_stage + off, q.src, q.bytes);
     PDLP_CUDA(cudaMemcpyAsync(q.dst, b->h_stage + off, q.bytes, cudaMemcpyHostToDevice, st));
-    off += (q.bytes + 15) / 16 * 16;
+    off += up16(q.bytes);
   }
-  PDLP_CUDA(cudaMemsetAsync(b->d_gcounters, 0, groups.size() * sizeof(unsigned), st));
+  if (b_rt) PDLP_CUDA(cudaMemcpyAsync(b->d_rtiles, srt, b_rt, cudaMemcpyHostToDevice, st));
+  if (b_ct) PDLP_CUDA(cudaMemcpyAsync(b->d_ctiles, sct, b_ct, cudaMemcpyHostToDevice, st));
+  if (b_gr) PDLP_CUDA(cudaMemcpyAsync(b->d_group_tiles, sgr, b_gr, cudaMemcpyHostToDevice, st));
+  PDLP_CUDA(cudaMemcpyAsync(b->d_inst, sin, b_in, cudaMemcpyHostToDevice, st));
+  PDLP_CUDA(cudaMemsetAsync(b->d_gcounters, 0, ngr * sizeof(unsigned), st));
   PDLP_CUDA(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * 2 * b->slots.size(), st));
   b->dirty = false;
   b->graph_stale = true;

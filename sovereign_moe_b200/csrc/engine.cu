@@ -4,6 +4,7 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <thread>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -1097,6 +1098,8 @@ bool tune_lookup(int m, int n, long long nnz, pdlp_tuning* out) {
 // (descriptor, tiles, initial state) or gives the arena back.
 
 struct Pending {
+  bool ptrs_ok = false;            // pointer arrays checked (host, before the enqueue)
+  int tile_rows = 0, tile_nnz = 0; // the tile shape admit_complete chose
   int slot = -1;
   void* arena = nullptr;
   size_t arena_bytes = 0;
@@ -1134,16 +1137,41 @@ static int admit_args(pdlp_batch* b, const pdlp_problem_desc* P, const pdlp_para
 // Phase 1.  pd.P, pd.prm, pd.rp and pd.cp are set by the caller (the pointer
 // arrays already readable on the host).  On success the slot is reserved,
 // the arena taken and the copies and the check enqueued on the stream.
+// The compressed pointers start at 0, do not decrease and end at nnz.
+static bool pointers_ok(const int64_t* p, int len, long long nnz) {
+  if (p[0] != 0 || p[len] != nnz) return false;
+  for (int i = 0; i < len; ++i) if (p[i + 1] < p[i]) return false;
+  return true;
+}
+
+// Runs fn(i) for i in [0, n) on up to 16 host threads: the admission's
+// per-LP host loops (pointer checks, tile planning) touch only that LP.
+template <class F>
+static void parallel_for(int n, F fn) {
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int T = std::min({n, hw, 16});
+  if (T <= 1) {
+    for (int i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::vector<std::thread> pool;
+  pool.reserve(T);
+  int started = 0;
+  try {
+    for (; started < T; ++started)
+      pool.emplace_back([&fn, started, T, n] { for (int i = started; i < n; i += T) fn(i); });
+  } catch (...) {                 // no thread could be started: this thread does the rest
+    for (int t = started; t < T; ++t)
+      for (int i = t; i < n; i += T) fn(i);
+  }
+  for (auto& th : pool) th.join();
+}
+
 static int admit_enqueue(pdlp_batch* b, Pending& pd, AdmitBatch& ab) {
   const pdlp_problem_desc* P = pd.P;
   const int m = P->m, n = P->n;
   const long long nnz = P->nnz;
-  auto check_ptr = [&](const int64_t* p, int len) {
-    if (p[0] != 0 || p[len] != nnz) return false;
-    for (int i = 0; i < len; ++i) if (p[i + 1] < p[i]) return false;
-    return true;
-  };
-  if (!check_ptr(pd.rp, m) || !check_ptr(pd.cp, n))
+  if (!pd.ptrs_ok)
     return fail(PDLP_ERR_ARG, "malformed compressed pointers (must start at 0, be non-decreasing and end at nnz)");
   int slot = -1;
   for (size_t s = 0; s < b->slots.size(); ++s)
@@ -1381,8 +1409,8 @@ static int admit_complete(pdlp_batch* b, Pending& pd, int herr) {
   I.check_every = prm.check_every; I.stepsize_every = prm.stepsize_every;
   I.beta_s = prm.beta_sufficient; I.beta_n = prm.beta_necessary; I.beta_a = prm.beta_artificial;
   I.theta = prm.primal_weight_smoothing;
-  plan_tiles(pd.rp, m, slot, tile_rows, tile_nnz, S.rt, S.rtw);
-  plan_tiles(pd.cp, n, slot, tile_rows, tile_nnz, S.ct, S.ctw);
+  pd.tile_rows = tile_rows;          // the tiles are planned by admit_many, in parallel
+  pd.tile_nnz = tile_nnz;
   // algorithmic bytes of one PDHG iteration: value + index per
   // entry and pointer per row on both passes, one gathered word per column /
   // row, the vectors each pass reads and writes
@@ -1462,6 +1490,11 @@ static int admit_many(pdlp_batch* b, int count, const pdlp_problem_desc* const* 
     }
   }
   if (need) PDLP_CUDA(cudaStreamSynchronize(st));
+  parallel_for(count, [&](int i) {
+    if (code[i] == PDLP_OK)
+      pd[i].ptrs_ok = pointers_ok(pd[i].rp, probs[i]->m, probs[i]->nnz) &&
+                      pointers_ok(pd[i].cp, probs[i]->n, probs[i]->nnz);
+  });
   AdmitBatch ab;
   for (int i = 0; i < count; ++i) {
     if (code[i] != PDLP_OK) continue;
@@ -1500,6 +1533,12 @@ static int admit_many(pdlp_batch* b, int count, const pdlp_problem_desc* const* 
     if (code[i] != PDLP_OK) continue;
     note(i, admit_complete(b, pd[i], b->h_errs[i]));
   }
+  parallel_for(count, [&](int i) {
+    if (code[i] != PDLP_OK) return;
+    Slot& S = b->slots[pd[i].slot];
+    plan_tiles(pd[i].rp, probs[i]->m, pd[i].slot, pd[i].tile_rows, pd[i].tile_nnz, S.rt, S.rtw);
+    plan_tiles(pd[i].cp, probs[i]->n, pd[i].slot, pd[i].tile_rows, pd[i].tile_nnz, S.ct, S.ctw);
+  });
   PDLP_CUDA(cudaStreamSynchronize(st));    // the initial states have left h_init
   for (int i = 0; i < count; ++i) {
     if (slots) slots[i] = code[i] == PDLP_OK ? pd[i].slot : -1;

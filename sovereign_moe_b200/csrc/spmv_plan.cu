@@ -33,11 +33,14 @@
 // bits):
 //   * a row of at most kLaneRow entries: one lane, storage order, each product
 //     rounded before it is added -- the order of the reference's CPU kernel
-//     (src/sovopt/core/sparse.py:50-58), so these rows equal it bit for bit;
+//     (src/sovopt/core/sparse.py:50-58), so these rows equal it bit for bit
+//     (the plan orders a tile's rows so that a warp's 32 rows start on
+//     different shared-memory banks);
 //   * a longer row of a normal tile: lane l sums entries l, l+32, ... in
 //     order, then a xor butterfly over the warp;
-//   * a huge row: the first consumer warp alone, read from global memory, in
-//     the same lane-strided order as a longer row.
+//   * a huge row: one warp (the first of the group that takes the tile),
+//     read from global memory, in the same lane-strided order as a longer
+//     row.
 //
 // Every wait on an mbarrier is bounded in wall time (kPlanWaitNs).  A wait
 // that runs out records PDLP_ERR_BARRIER_TIMEOUT in the plan's status word

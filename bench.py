@@ -334,7 +334,7 @@ class GpuArm:
         res = (L.Result * n)()
         ptrs = [(ct.c_void_p * n)(*[o[j].data_ptr() for o in outs]) for j in range(3)]
         L.check(c.pdlp_batch_collect_many(self.eng.h, n, (ct.c_int32 * n)(*slots), res,
-                                          ptrs[0], ptrs[1], ptrs[2], mem, 1))
+                                          ptrs[0], ptrs[1], ptrs[2], None, mem, 1))
         statuses, starts, ends, self.per_lp = [], [], [], []
         for r, k in zip(res, self.lps):
             statuses.append(r.status)
@@ -371,7 +371,7 @@ class GpuArm:
             r = L.Result()
             one = lambda a: (ct.c_void_p * 1)(a.data_ptr())  # noqa: E731
             L.check(c.pdlp_batch_collect_many(h, 1, (ct.c_int32 * 1)(s.value), ct.byref(r),
-                                              one(x), one(y), one(dd), L.PDLP_MEM_HOST, 1))
+                                              one(x), one(y), one(dd), None, L.PDLP_MEM_HOST, 1))
             if r.status != 0:
                 raise RuntimeError(f"one-at-a-time solve ended with status {r.status}")
             service.append(time.perf_counter() - t0)

@@ -243,16 +243,16 @@ int pdlp_batch_statuses(pdlp_batch* b, int32_t* status_out, int32_t n);
  * pdlp_batch_destroy. */
 int pdlp_batch_retire(pdlp_batch* b, int32_t slot);
 /* Poll, fetch and (when retire != 0) retire n finished slots at once: their
- * results into results[0..n) (optional), x[i], y[i], d[i] as
+ * results into results[0..n) (optional), x[i], y[i], d[i] and history[i] as
  * pdlp_batch_fetch writes them (each pointer array optional, each entry may be
  * NULL), with one synchronisation of the batch's stream for the whole set
- * instead of three per slot.  A running, free or repeated slot is refused
+ * (two when histories are fetched) instead of three per slot.  A running, free or repeated slot is refused
  * (PDLP_ERR_STATE / PDLP_ERR_ARG) before anything is copied.  No counterpart
  * in the reference, which solves one LP per call; it is the collecting side
  * of pdlp_batch_admit_many. */
 int pdlp_batch_collect_many(pdlp_batch* b, int32_t n, const int32_t* slots, pdlp_result* results,
                             double* const* x, double* const* y, double* const* d,
-                            int32_t memory, int32_t retire);
+                            double* const* history, int32_t memory, int32_t retire);
 /* Requests the slot to stop at its next check (status INTERRUPTED). */
 int pdlp_batch_cancel(pdlp_batch* b, int32_t slot);
 /* The slot's preconditioner, the reference's Scaling (src/sovopt/numerics/

@@ -153,8 +153,8 @@ SIGNATURES = {
     "pdlp_batch_poll": ([_c_p, _i32, ctypes.POINTER(Result)], ctypes.c_int),
     "pdlp_batch_fetch": ([_c_p, _i32, _c_p, _c_p, _c_p, _c_p, _i32], ctypes.c_int),
     "pdlp_batch_retire": ([_c_p, _i32], ctypes.c_int),
-    "pdlp_batch_collect_many": ([_c_p, _i32, _c_p, ctypes.POINTER(Result), _c_p, _c_p, _c_p, _i32,
-                                 _i32], ctypes.c_int),
+    "pdlp_batch_collect_many": ([_c_p, _i32, _c_p, ctypes.POINTER(Result), _c_p, _c_p, _c_p, _c_p,
+                                 _i32, _i32], ctypes.c_int),
     "pdlp_batch_statuses": ([_c_p, _c_p, _i32], ctypes.c_int),
     "pdlp_batch_cancel": ([_c_p, _i32], ctypes.c_int),
     "pdlp_batch_scaling": ([_c_p, _i32, _c_p, _c_p, ctypes.POINTER(_d), _i32], ctypes.c_int),

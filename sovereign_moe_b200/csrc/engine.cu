@@ -1946,7 +1946,7 @@ int pdlp_batch_poll(pdlp_batch* b, int32_t slot, pdlp_result* r) {
 
 int pdlp_batch_collect_many(pdlp_batch* b, int32_t n, const int32_t* slots, pdlp_result* results,
                             double* const* x, double* const* y, double* const* d,
-                            int32_t memory, int32_t retire) {
+                            double* const* history, int32_t memory, int32_t retire) {
   if (!b || n < 0 || (n > 0 && !slots)) return fail(PDLP_ERR_ARG, "NULL argument");
   if (memory != PDLP_MEM_HOST && memory != PDLP_MEM_DEVICE)
     return fail(PDLP_ERR_ARG, "memory must be PDLP_MEM_HOST or PDLP_MEM_DEVICE");
@@ -1971,6 +1971,18 @@ int pdlp_batch_collect_many(pdlp_batch* b, int32_t n, const int32_t* slots, pdlp
     if (d && d[i] && sl.n) PDLP_CUDA(cudaMemcpyAsync(d[i], sl.inst.dout, sizeof(double) * sl.n, k, st));
   }
   PDLP_CUDA(cudaStreamSynchronize(st));
+  if (history) {                    // each slot's check history, now that its length is known
+    bool any = false;
+    for (int32_t i = 0; i < n; ++i) {
+      const Slot& sl = b->slots[slots[i]];
+      const int len = std::min(b->h_state[slots[i]].hist_len, sl.inst.hist_cap);
+      if (history[i] && len > 0) {
+        PDLP_CUDA(cudaMemcpyAsync(history[i], sl.inst.hist, sizeof(double) * 5 * (size_t)len, k, st));
+        any = true;
+      }
+    }
+    if (any) PDLP_CUDA(cudaStreamSynchronize(st));
+  }
   for (int32_t i = 0; i < n; ++i)
     if (results) result_of(b->h_state[slots[i]], results + i);
   if (retire) {

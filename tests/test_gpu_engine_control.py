@@ -209,7 +209,7 @@ def test_collect_many_equals_poll_fetch_retire(require_gpu):
         lib = eng.lib
         n = len(slots)
         arr = (ctypes.c_int32 * n)(*slots)
-        assert lib.pdlp_batch_collect_many(eng.h, n, arr, None, None, None, None,
+        assert lib.pdlp_batch_collect_many(eng.h, n, arr, None, None, None, None, None,
                                            _lib.PDLP_MEM_HOST, 0) == _lib.PDLP_ERR_STATE
         eng.run()
         ref = [eng.fetch(s) for s in slots]
@@ -219,18 +219,22 @@ def test_collect_many_equals_poll_fetch_retire(require_gpu):
         ds = [np.full(p.A.n, np.nan) for p in probs]
         ptr = lambda vs: (ctypes.c_void_p * n)(*[v.ctypes.data for v in vs])  # noqa: E731
         twice = (ctypes.c_int32 * 2)(slots[0], slots[0])
-        assert lib.pdlp_batch_collect_many(eng.h, 2, twice, None, None, None, None,
+        assert lib.pdlp_batch_collect_many(eng.h, 2, twice, None, None, None, None, None,
                                            _lib.PDLP_MEM_HOST, 1) == _lib.PDLP_ERR_ARG
         res = (_lib.Result * n)()
-        assert lib.pdlp_batch_collect_many(eng.h, n, arr, res, ptr(xs), ptr(ys), ptr(ds),
+        hs = [np.full(5 * max(eng._meta[s][2], 1), np.nan) for s in slots]
+        assert lib.pdlp_batch_collect_many(eng.h, n, arr, res, ptr(xs), ptr(ys), ptr(ds), ptr(hs),
                                            _lib.PDLP_MEM_HOST, 1) == 0
         for i in range(n):
             assert bytes(res[i]) == bytes(polls[i])
             assert np.array_equal(xs[i], ref[i].x) and np.array_equal(ys[i], ref[i].y)
             assert np.array_equal(ds[i], ref[i].reduced_costs)
+            hl = res[i].history_len
+            assert hl == len(ref[i].log) and np.array_equal(
+                hs[i][:5 * hl].reshape(-1, 5), np.array(ref[i].log, dtype=float).reshape(-1, 5))
         # retired: the slots are free, and a new admission reuses an arena
         assert lib.pdlp_batch_collect_many(eng.h, 1, (ctypes.c_int32 * 1)(slots[0]), None, None,
-                                           None, None, _lib.PDLP_MEM_HOST, 1) == _lib.PDLP_ERR_ARG
+                                           None, None, None, _lib.PDLP_MEM_HOST, 1) == _lib.PDLP_ERR_ARG
         assert list(eng.statuses()[:8]).count(_lib.PDLP_SLOT_FREE) == 8
         again, codes = eng.admit_many(probs[:2], P6)
         assert codes == [0, 0]

@@ -213,7 +213,11 @@ int pdlp_batch_admit(pdlp_batch* b, const pdlp_problem_desc* prob,
 /* Admits `count` LPs (arrays of descriptors and parameters; params NULL for
  * the defaults) with three host synchronisations in all instead of two per
  * LP: one for the device pointer arrays (only when an LP is in device
- * memory), one for the device checks' verdicts and one at the end.
+ * memory), one for the device checks' verdicts and one at the end.  The
+ * device work of the whole call is two launches: one kernel copies every
+ * device-resident input into the slots (an array declared PDLP_MEM_DEVICE
+ * must be device or managed memory, else PDLP_ERR_ARG), one validates every
+ * LP's arrays.
  * slots_out[i] and codes_out[i] (each optional) receive each LP's slot (-1
  * when refused) and code; a refused LP leaves the others admitted.  Returns
  * the first refusal's code (its message in pdlp_last_error) or PDLP_OK.

@@ -29,6 +29,15 @@
 // So the matrix streams from HBM while earlier tiles are being summed, and
 // the gathers of x read shared memory instead of one L1 wavefront each.
 //
+// Each product is launched as a programmatic dependent of the kernel before
+// it in the stream.  Its CTAs take an SM as the previous kernel's CTAs leave
+// it, and copy the descriptors and the plan's arrays (row order, row
+// pointers, indices) of their first kPlanStages tiles.  Only after the
+// previous kernel has completed (griddepcontrol.wait) do they read the
+// caller's values and x or write y.  In a loop of products this hides the
+// launch and the first copies of each product behind the tail of the one
+// before.
+//
 // Summation order (fixed by the matrix alone, so repeated calls give the same
 // bits):
 //   * a row of at most kLaneRow entries: one lane, storage order, each product
@@ -171,6 +180,19 @@ __device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
+// Programmatic dependent launch.  grid_dep_wait returns once the kernel
+// before this one in the stream has completed and its writes are visible (at
+// once when there is none); grid_dep_release lets the next kernel in the
+// stream, if it was launched as a programmatic dependent, start its CTAs as
+// this kernel's CTAs leave the SMs.
+__device__ __forceinline__ void grid_dep_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+__device__ __forceinline__ void grid_dep_release() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Waits for the phase of `bar` with parity `parity`; false (and the status
 // word set) once kPlanWaitNs of wall time have passed.
 __device__ bool plan_wait(unsigned long long* bar, unsigned parity, int* status) {
@@ -304,17 +326,70 @@ __global__ void __launch_bounds__(kPlanThreads, 1) spmv_plan_kernel(
     mbar_init_fence();
   }
   __syncthreads();
+  // Every CTA of this kernel is resident from here on, so the next product
+  // may start its CTAs as these leave.  Until grid_dep_wait returns, a CTA
+  // reads only the plan's own arrays (uploaded before plan creation
+  // returned): the caller's values, x and y are touched after it.
+  grid_dep_release();
 
   if (warp == kCopyWarp) {
-    // the lanes fetch 32 tile descriptors at once; lane 0 waits for each
-    // stage to be free, writes the descriptor into it and issues the copies
-    int k = 0;
+    // lane 0 writes a tile's descriptor into its stage and issues its copies:
+    // first those of the plan's arrays (row order, row pointers, indices),
+    // then those of the caller's values and x window
+    auto stage_plan = [&](const PlanTile& t, int s) {
+      unsigned char* st = smem + s * L::bytes;
+      *reinterpret_cast<PlanTile*>(st) = t;       // published by the arrive below
+      // the consumers' reads of this stage (generic proxy) come before the
+      // copy engine's writes into it (async proxy)
+      fence_proxy_async();
+      if (t.kind == TILE_HUGE) {                  // read from global memory by a consumer warp
+        mbar_arrive(&full[s]);
+        return;
+      }
+      const unsigned bperm = lbulk_bytes<2>(t.r0, t.nshort);
+      const unsigned brp = lbulk_bytes<8>(t.r0, t.nr + 1);
+      const unsigned bidx = lbulk_bytes<4>(t.p0, t.cnt);
+      const unsigned bval = lbulk_bytes<(int)sizeof(T)>(base + t.p0, t.cnt);
+      const unsigned bx = lbulk_bytes<(int)sizeof(T)>(t.blo, t.bcnt);
+      // the phase completes when all five copies have landed
+      mbar_arrive_tx(&full[s], bperm + brp + bidx + bval + bx);
+      lbulk_stage<2>(st + L::perm_off, perm, t.r0, bperm, &full[s]);
+      lbulk_stage<8>(st + L::rp_off, rp, t.r0, brp, &full[s]);
+      lbulk_stage<4>(st + L::idx_off, idx, t.p0, bidx, &full[s]);
+    };
+    auto stage_caller = [&](const PlanTile& t, int s) {
+      if (t.kind == TILE_HUGE) return;
+      unsigned char* st = smem + s * L::bytes;
+      lbulk_stage<(int)sizeof(T)>(st + L::val_off, rx, base + t.p0,
+                                  lbulk_bytes<(int)sizeof(T)>(base + t.p0, t.cnt), &full[s]);
+      lbulk_stage<(int)sizeof(T)>(st + L::x_off, x, t.blo,
+                                  lbulk_bytes<(int)sizeof(T)>(t.blo, t.bcnt), &full[s]);
+    };
+    // the first kPlanStages tiles (free stages): the plan's part while the
+    // kernel before this one may still run, the caller's part after it ends
+    PlanTile mine{};
+    if (lane < count) mine = tiles[t_begin + lane];
+    const int primed = min(count, kPlanStages);
+    for (int j = 0; j < primed; ++j) {
+      const PlanTile t = shfl_tile(mine, j);
+      if (lane == 0) stage_plan(t, j);
+    }
+    grid_dep_wait();
+    for (int j = 0; j < primed; ++j) {
+      const PlanTile t = shfl_tile(mine, j);
+      if (lane == 0) stage_caller(t, j);
+    }
+    // the rest: the lanes fetch 32 tile descriptors at once; lane 0 waits for
+    // each stage to be free, then stages the tile
+    int k = primed;
     bool stop = false;
     for (int c0 = 0; c0 < count && !stop; c0 += kChunk) {
-      PlanTile mine{};
-      if (c0 + lane < count) mine = tiles[t_begin + c0 + lane];
+      if (c0 > 0) {
+        mine = PlanTile{};
+        if (c0 + lane < count) mine = tiles[t_begin + c0 + lane];
+      }
       const int cn = min(kChunk, count - c0);
-      for (int j = 0; j < cn; ++j, ++k) {
+      for (int j = c0 == 0 ? primed : 0; j < cn; ++j, ++k) {
         const int s = k % kPlanStages;
         int go = 1;
         if (lane == 0) {
@@ -325,26 +400,8 @@ __global__ void __launch_bounds__(kPlanThreads, 1) spmv_plan_kernel(
         if (!go) { stop = true; break; }
         const PlanTile t = shfl_tile(mine, j);
         if (lane == 0) {
-          unsigned char* st = smem + s * L::bytes;
-          *reinterpret_cast<PlanTile*>(st) = t;     // published by the arrive below
-          // the consumers' reads of this stage (generic proxy) come before
-          // the copy engine's writes into it (async proxy)
-          fence_proxy_async();
-          if (t.kind == TILE_HUGE) {              // read from global memory by a consumer warp
-            mbar_arrive(&full[s]);
-          } else {
-            const unsigned bperm = lbulk_bytes<2>(t.r0, t.nshort);
-            const unsigned brp = lbulk_bytes<8>(t.r0, t.nr + 1);
-            const unsigned bidx = lbulk_bytes<4>(t.p0, t.cnt);
-            const unsigned bval = lbulk_bytes<(int)sizeof(T)>(base + t.p0, t.cnt);
-            const unsigned bx = lbulk_bytes<(int)sizeof(T)>(t.blo, t.bcnt);
-            mbar_arrive_tx(&full[s], bperm + brp + bidx + bval + bx);
-            lbulk_stage<2>(st + L::perm_off, perm, t.r0, bperm, &full[s]);
-            lbulk_stage<8>(st + L::rp_off, rp, t.r0, brp, &full[s]);
-            lbulk_stage<4>(st + L::idx_off, idx, t.p0, bidx, &full[s]);
-            lbulk_stage<(int)sizeof(T)>(st + L::val_off, rx, base + t.p0, bval, &full[s]);
-            lbulk_stage<(int)sizeof(T)>(st + L::x_off, x, t.blo, bx, &full[s]);
-          }
+          stage_plan(t, s);
+          stage_caller(t, s);
         }
       }
     }
@@ -373,6 +430,7 @@ __global__ void __launch_bounds__(kPlanThreads, 1) spmv_plan_kernel(
         hcols[j][lane] = (j < cn && lane < nh) ? __ldg(halo_cols + hf + lane) : -1;
       }
       __syncwarp();
+      if (c0 == 0) grid_dep_wait();          // x is the caller's
       int col = hcols[0][lane];
       T cur = col >= 0 ? __ldg(x + col) : T(0);
       for (int j = 0; j < cn; ++j, ++k) {
@@ -398,7 +456,10 @@ __global__ void __launch_bounds__(kPlanThreads, 1) spmv_plan_kernel(
     return;
   }
 
-  // consumer warps: group g sums tiles g, g + kGroups, ...
+  // consumer warps: group g sums tiles g, g + kGroups, ...  (A stage fills
+  // only after the copy and halo warps' waits; the consumers wait too, since
+  // they read x and the values of huge tiles from global memory and write y.)
+  grid_dep_wait();
   const int group = warp / kGroupW, gw = warp % kGroupW;
   for (int k = group; k < count; k += kGroups) {
     const int s = k % kPlanStages;
@@ -727,11 +788,27 @@ int plan_run(pdlp_spmv_plan* p, const T* rx, const T* x, T* y, cudaStream_t st) 
   if (p->info.kernel == PDLP_SPMV_PLAN_STREAMED) return spmv_streamed(p, rx + p->base, x, y, st);
   if ((reinterpret_cast<uintptr_t>(rx) | reinterpret_cast<uintptr_t>(x)) & 15u)
     return fail(PDLP_ERR_ARG, "rx and x must be 16-byte aligned (bulk copies)");
-  spmv_plan_kernel<T><<<p->nctas, kPlanThreads, kPlanStages * StageLayout<T>::bytes, st>>>(
-      static_cast<const PlanTile*>(p->tiles), p->cta_first, p->rp, p->idx, rx, x, y,
-      p->long_rows, p->halo_cols, p->perm, p->base, p->status);
+  // launched as a programmatic dependent of the kernel before it in the
+  // stream: its CTAs stage the plan's arrays while that kernel drains
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(p->nctas);
+  cfg.blockDim = dim3(kPlanThreads);
+  cfg.dynamicSmemBytes = kPlanStages * StageLayout<T>::bytes;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  PDLP_CUDA(cudaLaunchKernelEx(&cfg, spmv_plan_kernel<T>, static_cast<const PlanTile*>(p->tiles),
+                               static_cast<const int*>(p->cta_first),
+                               static_cast<const int64_t*>(p->rp),
+                               static_cast<const int*>(p->idx), rx, x, y,
+                               static_cast<const int*>(p->long_rows),
+                               static_cast<const int*>(p->halo_cols),
+                               static_cast<const uint16_t*>(p->perm), (long long)p->base,
+                               p->status));
   count_launches(1);
-  PDLP_CUDA(cudaGetLastError());
   return PDLP_OK;
 }
 

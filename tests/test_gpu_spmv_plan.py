@@ -273,3 +273,77 @@ def test_plan_rejects_bad_structure(bk):
     assert "out of range" in bk.lib.pdlp_last_error().decode()
     assert bk.lib.pdlp_spmv_plan_create(-1, 4, None, None, st, ctypes.byref(h)) == _lib.PDLP_ERR_ARG
     assert bk.lib.pdlp_spmv_plan_run_f64(None, None, None, None, st) == _lib.PDLP_ERR_ARG
+
+
+def _rounded(v, f32):
+    """The values as the float32 kernel sees them (the oracle takes float64)."""
+    return v.astype(np.float32).astype(np.float64) if f32 else v
+
+
+@pytest.mark.parametrize("f32", [False, True])
+def test_back_to_back_products_keep_stream_order(bk, f32):
+    """Products launched back to back, each a programmatic dependent of the
+    kernel before it (its CTAs stage the plan's arrays while that kernel
+    drains): the chain w = A u, u = A^T w, ... reads the previous product's
+    output (read after write) and overwrites the vector the previous product
+    read (write after read), with a torch kernel between two of the steps.
+    Run with a synchronisation after every step, each step equals the oracle
+    on its input; run with none, three times over, the chain ends on the
+    same bits."""
+    import torch
+    from sovereign_moe_b200.workloads import blending_plan
+    S = blending_plan(seed=5, m=20_000, n=60_000, periods=72).problem.A
+    A, At = Csr.of(S), Csr.transpose_of(S)
+    dt = torch.float32 if f32 else torch.float64
+    pa = bk.spmv_plan(bk.pointer(A.rp), bk.index(A.ri), A.m, A.n)
+    pt = bk.spmv_plan(bk.pointer(At.rp), bk.index(At.ri), At.m, At.n)
+    assert pa.info()["kernel"] == 0 and pt.info()["kernel"] == 0
+    ax, atx = bk.to_device(A.rx).to(dt), bk.to_device(At.rx).to(dt)
+    u0 = bk.to_device(np.random.default_rng(6).standard_normal(A.n)).to(dt)
+
+    def chain(u, w, sync):
+        snaps = []
+        for step in range(6):
+            if step % 2 == 0:
+                bk.spmv_planned(pa, ax, u, w)
+            else:
+                bk.spmv_planned(pt, atx, w, u)
+                if step == 1:
+                    u.mul_(0.125)                  # exact: a power of two
+            if sync:
+                torch.cuda.synchronize()
+                snaps.append((u.clone(), w.clone()))
+        return snaps
+
+    u = u0.clone()
+    w = torch.full((A.m,), POISON, dtype=dt, device="cuda")
+    snaps = chain(u, w, sync=True)
+    assert pa.status(bk._stream()) == 0 and pt.status(bk._stream()) == 0
+    prev_u = u0.cpu().numpy().astype(np.float64)
+    short = _short_rows(A)
+    for step, (su, sw) in enumerate(snaps):
+        su, sw = su.cpu().numpy().astype(np.float64), sw.cpu().numpy().astype(np.float64)
+        if step % 2 == 0:
+            exp = po.spmv(A.rp, A.ri, _rounded(A.rx, f32), prev_u)
+            if f32:
+                np.testing.assert_allclose(sw, exp, rtol=1e-4, atol=1e-3 * np.abs(exp).max())
+            else:
+                np.testing.assert_allclose(sw, exp, rtol=1e-12, atol=1e-12)
+                assert np.array_equal(sw[short], exp[short])
+        else:
+            exp = po.spmv(At.rp, At.ri, _rounded(At.rx, f32), sw)
+            exp = exp * 0.125 if step == 1 else exp
+            if f32:
+                np.testing.assert_allclose(su, exp, rtol=1e-4, atol=1e-3 * np.abs(exp).max())
+            else:
+                assert np.array_equal(su, exp)      # every column of A has 5 entries
+            prev_u = su
+    want_u, want_w = snaps[-1]
+    for _ in range(3):
+        u = u0.clone()
+        w = torch.full((A.m,), POISON, dtype=dt, device="cuda")
+        torch.cuda.synchronize()
+        chain(u, w, sync=False)
+        torch.cuda.synchronize()
+        assert torch.equal(u, want_u) and torch.equal(w, want_w)
+    assert pa.status(bk._stream()) == 0 and pt.status(bk._stream()) == 0

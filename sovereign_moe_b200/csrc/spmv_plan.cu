@@ -31,10 +31,10 @@
 //
 // Each product is launched as a programmatic dependent of the kernel before
 // it in the stream.  Its CTAs take an SM as the previous kernel's CTAs leave
-// it, and copy the descriptors and the plan's arrays (row order, row
-// pointers, indices) of their first kPlanStages tiles.  Only after the
-// previous kernel has completed (griddepcontrol.wait) do they read the
-// caller's values and x or write y.  In a loop of products this hides the
+// it, fetch their tile descriptors and copy the plan's arrays (row order,
+// row pointers, indices) of the first tile of each consumer group.  Only
+// after the previous kernel has completed (griddepcontrol.wait) do they read
+// the caller's values and x or write y.  In a loop of products this hides the
 // launch and the first copies of each product behind the tail of the one
 // before.
 //
@@ -365,16 +365,22 @@ __global__ void __launch_bounds__(kPlanThreads, 1) spmv_plan_kernel(
       lbulk_stage<(int)sizeof(T)>(st + L::x_off, x, t.blo,
                                   lbulk_bytes<(int)sizeof(T)>(t.blo, t.bcnt), &full[s]);
     };
-    // the first kPlanStages tiles (free stages): the plan's part while the
-    // kernel before this one may still run, the caller's part after it ends
+    // the first tile of each consumer group (free stages): the plan's part
+    // while the kernel before this one may still run, the caller's part after
+    // it ends.  (Priming all kPlanStages stages put the plan's copies of
+    // later tiles ahead of the first tile's values in a single call, about
+    // 1 us later to its end.)
     PlanTile mine{};
     if (lane < count) mine = tiles[t_begin + lane];
-    const int primed = min(count, kPlanStages);
+    const int primed = min(count, kGroups);
     for (int j = 0; j < primed; ++j) {
       const PlanTile t = shfl_tile(mine, j);
       if (lane == 0) stage_plan(t, j);
     }
     grid_dep_wait();
+    // the previous kernel's ordinary stores to the values and x come before
+    // this lane's bulk (async proxy) reads of them
+    if (lane == 0) fence_proxy_async_global();
     for (int j = 0; j < primed; ++j) {
       const PlanTile t = shfl_tile(mine, j);
       if (lane == 0) stage_caller(t, j);

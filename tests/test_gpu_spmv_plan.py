@@ -347,3 +347,32 @@ def test_back_to_back_products_keep_stream_order(bk, f32):
         torch.cuda.synchronize()
         assert torch.equal(u, want_u) and torch.equal(w, want_w)
     assert pa.status(bk._stream()) == 0 and pt.status(bk._stream()) == 0
+
+
+def test_product_after_copies_into_its_inputs(bk):
+    """A product launched right after asynchronous copies into its own
+    inputs (x from pinned host memory, the values from another device
+    buffer, no synchronisation in between) reads the copied data: the
+    dependency on a copy is a full one, like the one on a kernel."""
+    import torch
+    A, rng = _matrix(np.random.default_rng(31).choice([2, 6, 15, 40], 5000), 12000, seed=32,
+                     banded=True)
+    plan = bk.spmv_plan(bk.pointer(A.rp), bk.index(A.ri), A.m, A.n)
+    assert plan.info()["kernel"] == 0
+    rx_dev = torch.zeros(A.nnz, dtype=torch.float64, device="cuda")
+    x_dev = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    out = torch.full((A.m,), POISON, dtype=torch.float64, device="cuda")
+    rx_src = bk.to_device(A.rx)
+    for trial in range(3):
+        x = rng.standard_normal(A.n)
+        x_host = torch.from_numpy(x).pin_memory()
+        torch.cuda.synchronize()
+        x_dev.copy_(x_host, non_blocking=True)
+        rx_dev.copy_(rx_src * float(trial + 1), non_blocking=True)
+        bk.spmv_planned(plan, rx_dev, x_dev, out)
+        torch.cuda.synchronize()
+        exp = po.spmv(A.rp, A.ri, A.rx * float(trial + 1), x)
+        short = _short_rows(A)
+        assert np.array_equal(out.cpu().numpy()[short], exp[short])
+        np.testing.assert_allclose(out.cpu().numpy(), exp, rtol=1e-12, atol=1e-12)
+    assert plan.status(bk._stream()) == 0

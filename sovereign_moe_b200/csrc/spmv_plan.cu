@@ -99,6 +99,13 @@ constexpr int kGroups = kPlanCW / kGroupW;
 constexpr int kCopyWarp = kPlanCW, kHaloWarp = kPlanCW + 1;
 constexpr int kPlanThreads = (kPlanCW + 2) * 32;
 constexpr int kPlanStages = 4;
+// Consumers wait on a stage by phase parity, so each stage must always be
+// consumed by the same group: tile k + kPlanStages is then the next tile of
+// the group that consumed tile k, which waits for it only after it has
+// released tile k.  With groups not dividing the stages, another group could
+// reach the stage while tile k's phase is still open, match the parity of the
+// phase before it, and read a stale stage.
+static_assert(kPlanStages % kGroups == 0, "every stage consumed by one group");
 constexpr int kChunk = 32;            // tile descriptors a warp fetches at once
 constexpr long long kPlanWaitNs = 1000000000LL;
 // cost model of the CTA balance (ns): a round trip to global memory, one to

@@ -376,3 +376,33 @@ def test_product_after_copies_into_its_inputs(bk):
         assert np.array_equal(out.cpu().numpy()[short], exp[short])
         np.testing.assert_allclose(out.cpu().numpy(), exp, rtol=1e-12, atol=1e-12)
     assert plan.status(bk._stream()) == 0
+
+
+@pytest.mark.parametrize("f32", [False, True])
+def test_full_size_plan_many_tiles_per_cta(bk, f32):
+    """The 200k x 600k blending plan of the SpMV bench: about ten tiles per
+    CTA in each product, so every stage of the ring is reused over several
+    phases by its consumer group (a stage taken on a stale phase shows up
+    as wrong rows or as a wait that runs out).  Both products equal the
+    oracle (float64 rows of at most 64 entries bit for bit), and a second
+    run gives the same bits."""
+    import torch
+    from sovereign_moe_b200.workloads import blending_plan
+    S = blending_plan(seed=0).problem.A
+    assert (S.m, S.n) == (200_000, 600_000)
+    rng = np.random.default_rng(17)
+    for C, v in ((Csr.of(S), rng.standard_normal(S.n)), (Csr.transpose_of(S),
+                                                         rng.standard_normal(S.m))):
+        got, plan = _run(bk, C, v, f32=f32)
+        info = plan.info()
+        assert info["kernel"] == 0 and info["tiles"] >= 8 * info["ctas"]
+        exp = po.spmv(C.rp, C.ri, _rounded(C.rx, f32), v)
+        if f32:
+            np.testing.assert_allclose(got, exp, rtol=1e-4, atol=1e-3 * np.abs(exp).max())
+        else:
+            short = _short_rows(C)
+            assert np.array_equal(got[short], exp[short])
+            np.testing.assert_allclose(got, exp, rtol=1e-12, atol=1e-12)
+        again, _ = _run(bk, C, v, f32=f32, plan=plan)
+        assert np.array_equal(again, got)
+    torch.cuda.synchronize()

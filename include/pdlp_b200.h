@@ -385,10 +385,10 @@ int pdlp_spmv_tune_f32(int32_t m, const int64_t* rp, const int32_t* ri, const fl
  * cudaMalloc and torch allocations are).  When fewer than half the entries
  * fall in a window or halo, a run is the row-block kernel instead
  * (pdlp_spmv_ex_* with PDLP_SPMV_STREAMED on the plan's copy; no alignment
- * rule).  The kernel is launched as a programmatic dependent of the kernel
- * before it in `stream`: it may start staging the plan's own arrays while
- * that kernel drains, but reads rx and x and writes y only after it has
- * completed, so stream order holds as for any launch.
+ * rule).  The tile kernel is launched as a programmatic dependent of the
+ * kernel before it in `stream`: it may start staging the plan's own arrays
+ * while that kernel drains, but reads rx and x and writes y only after it
+ * has completed, so stream order holds as for any launch.
  * Asynchronous; repeated runs give the same bits.  A wait inside the
  * kernel that runs out (1 s) records PDLP_ERR_BARRIER_TIMEOUT, which
  * pdlp_spmv_plan_status returns (and clears) after synchronising `stream`. */

@@ -119,10 +119,10 @@ typedef struct pdlp_params {
     /* Scheduling hint (no counterpart in the reference): the caller's
      * estimate of the PDHG iterations this LP needs, 0 = none.  When every
      * running LP of a batch has one, the engine sizes their block teams by
-     * expected remaining work (work per iteration times the iterations left)
-     * instead of work per iteration, so that the LPs expected to run longest
-     * get their blocks first.  Results do not depend on it: an LP's bits are
-     * the same whichever warps run its tiles. */
+     * expected remaining work (work per iteration times the square root of
+     * the iterations left) instead of work per iteration, so that the LPs
+     * expected to run longest get more blocks.  Results do not depend on it:
+     * an LP's bits are the same whichever warps run its tiles. */
     double expected_iterations;
 } pdlp_params;
 

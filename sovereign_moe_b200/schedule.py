@@ -2,8 +2,8 @@
 
 How many PDHG iterations an LP needs varies by an order of magnitude within
 one batch, and the batch's makespan is set by the LPs that need the most.
-The engine can give those LPs their blocks first when each admitted LP
-carries an estimate (``pdlp_params.expected_iterations``).  ``IterationModel``
+The engine can give those LPs more blocks when each admitted LP carries an
+estimate (``pdlp_params.expected_iterations``).  ``IterationModel``
 supplies one: the median iteration count of the LPs already finished in the
 same shape class.  The class is the number of columns per row in half
 octaves, the shape feature that tracks the iteration count best on the

@@ -93,7 +93,7 @@ class Server:
         self.queue: deque = deque()
         self.inflight: dict = {}
         # iteration estimates learned from the requests served so far: the
-        # engine gives the LPs expected to run longest their blocks first
+        # engine gives the LPs expected to run longest more blocks
         self.model = IterationModel()
 
     def close(self):
